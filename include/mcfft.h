@@ -1,0 +1,130 @@
+/*
+ * mcfft.h -- C ABI of the B200 (sm_100a) batched complex-to-complex
+ * tensor-core FFT.
+ *
+ * This is the drop-in boundary.  The reference exports only C++-linkage
+ * entry points with no status returns and one global plan per process:
+ *   mcfftCreate(mcfftHandle*, int n, int n_batch)        include/mcfft_1d_device.h:38
+ *   mcfftCreate(mcfftHandle*, int nx, int ny, int n_batch) include/mcfft_2d_device.h:38
+ *   mcfftExec(mcfftHandle, MCTYPE* data)                 include/mcfft_1d_device.h:37
+ *   setup / doit / finalize / generate_data              include/mcfft_1d_utils.h:8-11
+ * Those keep their signatures in include/mcfft_{1d,2d,3d}_utils.h (compat
+ * shims over this ABI).  The functions below are the plan-based core every
+ * binding (C, C++, ctypes, cgo, JNI) calls: plain pointers and integers,
+ * status codes, no CUDA or framework types in the signatures (the stream is
+ * a cudaStream_t passed as void*).
+ *
+ * Data layout: interleaved complex (re, im), batch-major, row-major
+ * multi-dimensional arrays with the last dimension contiguous -- the
+ * reference's layout (source/mcfft_2d_utils.cpp:49-50).  Input and output
+ * are natural order (the reference required digit-reversed input,
+ * source/mcfft_1d_utils.cpp:43-59).
+ *
+ * Precision forms:
+ *   MCFFT_PREC_FP16   plain: FP16 in, FP16 out, FP32 accumulation, each
+ *                     radix-16 stage scaled by 1/16 (radix-R tail by 1/R),
+ *                     so out = DFT(in) * 2^scale_log2 with scale_log2 =
+ *                     -log2(number of points of one transform).
+ *   MCFFT_PREC_SPLIT  split hi+lo FP16 operands, three products per stage,
+ *                     FP32 accumulation: FP32 in (or FP16 in with
+ *                     MCFFT_FLAG_INPUT_F16), FP32 out, unnormalised DFT
+ *                     (scale_log2 = 0), like FFTW_FORWARD/FFTW_BACKWARD.
+ *
+ * Sizes: every dimension a power of two >= 16; 1D lengths up to 2^26 (two
+ * passes above 8192); 2D/3D sides up to 8192.
+ */
+#ifndef MCFFT_H_
+#define MCFFT_H_
+
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define MCFFT_API __attribute__((visibility("default")))
+#else
+#define MCFFT_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  MCFFT_SUCCESS = 0,
+  MCFFT_INVALID_PLAN = 1,
+  MCFFT_ALLOC_FAILED = 2,
+  MCFFT_INVALID_VALUE = 3,
+  MCFFT_UNSUPPORTED_SIZE = 4,
+  MCFFT_CUDA_ERROR = 5,
+  MCFFT_DEVICE_TIMEOUT = 6,
+  MCFFT_INTERNAL_ERROR = 7,
+  MCFFT_NO_DEVICE = 8
+} mcfftResult;
+
+typedef enum { MCFFT_PREC_FP16 = 0, MCFFT_PREC_SPLIT = 1 } mcfftPrecision;
+
+#define MCFFT_FORWARD (-1)
+#define MCFFT_INVERSE (1)
+
+/* Plan flags. */
+#define MCFFT_FLAG_NONE 0u
+/* Split form only: the input is FP16 complex instead of FP32. */
+#define MCFFT_FLAG_INPUT_F16 1u
+
+typedef struct mcfftPlan_st* mcfftPlan;
+
+/* One transform description for mcfftPlanCreateBatch. */
+typedef struct {
+  int ndim;          /* 1, 2 or 3 */
+  int64_t dims[3];   /* dims[0..ndim), last contiguous */
+  int64_t batch;     /* transforms of this shape */
+  int64_t in_offset; /* element offset of the first one in the input */
+  int64_t out_offset;/* element offset of the first one in the output */
+} mcfftDesc;
+
+/* Plan information. */
+typedef struct {
+  int ndim;
+  int64_t dims[3];
+  int64_t batch;
+  int precision;
+  int num_passes;          /* HBM passes per exec (kernel launches unless fused) */
+  int scale_log2;          /* out = DFT(in) * 2^scale_log2 */
+  int64_t elements;        /* complex elements per exec (all transforms) */
+  int64_t in_bytes;        /* bytes read from the input per exec */
+  int64_t out_bytes;       /* bytes written to the output per exec */
+  int64_t workspace_bytes; /* device scratch held by the plan */
+  int num_descs;           /* transform groups (mcfftPlanCreateBatch) */
+} mcfftPlanInfo;
+
+MCFFT_API mcfftResult mcfftPlanCreate1d(mcfftPlan* plan, int64_t n, int64_t batch,
+                              mcfftPrecision precision, unsigned flags);
+MCFFT_API mcfftResult mcfftPlanCreate2d(mcfftPlan* plan, int64_t nx, int64_t ny, int64_t batch,
+                              mcfftPrecision precision, unsigned flags);
+MCFFT_API mcfftResult mcfftPlanCreate3d(mcfftPlan* plan, int64_t nx, int64_t ny, int64_t nz,
+                              int64_t batch, mcfftPrecision precision, unsigned flags);
+/* Many transforms of uneven size/dimensionality executed together. */
+MCFFT_API mcfftResult mcfftPlanCreateBatch(mcfftPlan* plan, const mcfftDesc* descs, int count,
+                                 mcfftPrecision precision, unsigned flags);
+
+/* Stream-ordered; `in` and `out` are device pointers (may be equal for
+ * single-pass plans).  direction: MCFFT_FORWARD or MCFFT_INVERSE.  One plan
+ * must not run concurrently on two streams (its workspace is shared). */
+MCFFT_API mcfftResult mcfftExec(mcfftPlan plan, const void* in, void* out, int direction,
+                      void* stream);
+
+/* Reads back and clears the plan's device status word (synchronises the
+ * plan's last stream).  MCFFT_DEVICE_TIMEOUT if a kernel gave up waiting. */
+MCFFT_API mcfftResult mcfftPlanCheckStatus(mcfftPlan plan);
+
+MCFFT_API mcfftResult mcfftPlanGetInfo(mcfftPlan plan, mcfftPlanInfo* info);
+MCFFT_API mcfftResult mcfftPlanDestroy(mcfftPlan plan);
+MCFFT_API const char* mcfftGetErrorString(mcfftResult result);
+
+/* Library version as 10000*major + 100*minor + patch. */
+MCFFT_API int mcfftGetVersion(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MCFFT_H_ */

@@ -1,0 +1,58 @@
+"""Build the native library mcfft_b200/libmcfft.so (sm_100a) in-tree.
+
+    python -m mcfft_b200.build            # or: python mcfft_b200/build.py
+
+nvcc cross-compiles for sm_100a without a GPU.  Objects go to
+mcfft_b200/_build/, the shared library next to this file so that it
+travels with the source tree.
+"""
+from __future__ import annotations
+
+import concurrent.futures as cf
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, "csrc")
+BUILD = os.path.join(HERE, "_build")
+LIB = os.path.join(HERE, "libmcfft.so")
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O2",
+         "-Xcompiler", "-fvisibility=hidden", "--expt-relaxed-constexpr"]
+SOURCES = ["tables.cu", "pass_kernels.cu", "mcfft_api.cu"]
+HEADERS = ["sm100_ptx.cuh", "fft_pass.cuh", "fft_pass_split.cuh", "mcfft_internal.h"]
+
+
+def _stale(target: str, deps) -> bool:
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(d) > t for d in deps)
+
+
+def _compile(src: str, verbose: bool) -> str:
+    obj = os.path.join(BUILD, os.path.splitext(src)[0] + ".o")
+    deps = [os.path.join(CSRC, src)] + [os.path.join(CSRC, h) for h in HEADERS]
+    deps.append(os.path.join(HERE, "..", "include", "mcfft.h"))
+    if _stale(obj, deps):
+        cmd = [NVCC, *ARCH, *FLAGS, "-c", os.path.join(CSRC, src), "-o", obj]
+        if verbose:
+            cmd.insert(1, "-Xptxas=-v")
+        subprocess.run(cmd, check=True)
+    return obj
+
+
+def build(verbose: bool = False) -> str:
+    os.makedirs(BUILD, exist_ok=True)
+    with cf.ThreadPoolExecutor(max_workers=len(SOURCES)) as ex:
+        objs = list(ex.map(lambda s: _compile(s, verbose), SOURCES))
+    if _stale(LIB, objs):
+        subprocess.run([NVCC, *ARCH, "-shared", "-o", LIB, *objs, "-cudart", "static"],
+                       check=True)
+    return LIB
+
+
+if __name__ == "__main__":
+    print(build(verbose="-v" in sys.argv))

@@ -1,0 +1,63 @@
+// tables.cu -- FP64 generation of twiddle tables and of the real-embedded
+// 16-point DFT matrix, on the GPU, rounded once to their storage types.
+//
+// The reference builds its DFT matrix on the host with single-precision
+// cosf/sinf (source/mcfft_1d_device.cpp:776-785) and advances twiddles by
+// repeated complex multiplication (e.g. :119-123); here every entry is an
+// independent FP64 sincospi of an exact rational angle.
+#include <cuda_fp16.h>
+
+#include "mcfft_internal.h"
+
+namespace mcfft {
+
+__global__ void k_gen_twiddles(float2* dst, int64_t count, int mode, int64_t m1, int shift,
+                               int64_t modulus, int sign, double scale) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  int64_t e = mode == 0 ? (i / m1) * (i % m1) : (i << shift);
+  e %= modulus;
+  // angle = sign * 2*pi*e/modulus; sincospi takes it in units of pi.
+  double x = (2.0 * (double)e) / (double)modulus;
+  double s, c;
+  sincospi(x, &s, &c);
+  dst[i] = make_float2((float)(c * scale), (float)(sign * s * scale));
+}
+
+cudaError_t gen_twiddle_table(float2* dst, int64_t count, int mode, int64_t m1, int shift,
+                              int64_t modulus, int sign, double scale, cudaStream_t st) {
+  if (count <= 0) return cudaSuccess;
+  int threads = 256;
+  int64_t blocks = (count + threads - 1) / threads;
+  k_gen_twiddles<<<(unsigned)blocks, threads, 0, st>>>(dst, count, mode, m1, shift, modulus,
+                                                       sign, scale);
+  return cudaGetLastError();
+}
+
+// B[kk][j] with K index kk = 2n + ri (input point n, re/im) and N index
+// j = 2k + rj (output point k, re/im):
+//   rj = 0 (real out):  ri=0 -> cos,  ri=1 -> -sin
+//   rj = 1 (imag out):  ri=0 -> sin,  ri=1 ->  cos
+// where cos + i sin = exp(sign * 2 pi i k n / 16).  Stored N-row-major with
+// K contiguous in 8-element chunks: byte (j&7)*16 + (j>>3)*512 + (kk>>3)*128
+// + (kk&7)*2 -- the layout the stage kernels hand to tcgen05 as K-major B.
+__global__ void k_gen_dft16(__half* hi, __half* lo, int sign) {
+  int t = threadIdx.x;  // 0..1023
+  int j = t >> 5, kk = t & 31;
+  int k = j >> 1, rj = j & 1, n = kk >> 1, ri = kk & 1;
+  double s, c;
+  sincospi(2.0 * (double)((k * n) % 16) / 16.0, &s, &c);
+  s *= sign;
+  double val = ri == 0 ? (rj == 0 ? c : s) : (rj == 0 ? -s : c);
+  int off = ((j & 7) * 16 + (j >> 3) * 512 + (kk >> 3) * 128 + (kk & 7) * 2) / 2;
+  __half h = __double2half(val);
+  hi[off] = h;
+  if (lo) lo[off] = __double2half(val - (double)__half2float(h));
+}
+
+cudaError_t gen_dft16_embedding(void* hi, void* lo, int sign, cudaStream_t st) {
+  k_gen_dft16<<<1, 1024, 0, st>>>(static_cast<__half*>(hi), static_cast<__half*>(lo), sign);
+  return cudaGetLastError();
+}
+
+}  // namespace mcfft
