@@ -21,8 +21,9 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O2",
          "-Xcompiler", "-fvisibility=hidden", "--expt-relaxed-constexpr"]
-SOURCES = ["tables.cu", "pass_kernels.cu", "mcfft_api.cu"]
-HEADERS = ["sm100_ptx.cuh", "fft_pass.cuh", "fft_pass_split.cuh", "mcfft_internal.h"]
+SOURCES = ["tables.cu", "pass_kernels.cu", "tile_pass.cu", "layout.cpp", "mcfft_api.cu"]
+HEADERS = ["sm100_ptx.cuh", "fft_pass.cuh", "fft_pass_split.cuh", "fft_tile.cuh", "tile_pass.h",
+           "layout.h", "mcfft_internal.h"]
 
 
 def _stale(target: str, deps) -> bool:
@@ -44,6 +45,21 @@ def _compile(src: str, verbose: bool) -> str:
     return obj
 
 
+def _compat(dim: int) -> str:
+    """libmcfft_{dim}d.so: the reference's harness signatures over the C ABI."""
+    out = os.path.join(HERE, f"libmcfft_{dim}d.so")
+    src = os.path.join(CSRC, "compat.cu")
+    deps = [src, LIB] + [os.path.join(HERE, "..", "include", h) for h in
+                         ("mcfft.h", "common.h", f"mcfft_{dim}d_utils.h", f"mcfft_{dim}d_device.h")]
+    if _stale(out, deps):
+        obj = os.path.join(BUILD, f"compat_{dim}d.o")
+        subprocess.run([NVCC, *ARCH, *FLAGS, f"-DMCFFT_COMPAT_DIM={dim}", "-c", src, "-o", obj],
+                       check=True)
+        subprocess.run([NVCC, *ARCH, "-shared", "-o", out, obj, "-L" + HERE, "-lmcfft",
+                        "-Xlinker", "-rpath,$ORIGIN", "-cudart", "static"], check=True)
+    return out
+
+
 def build(verbose: bool = False) -> str:
     os.makedirs(BUILD, exist_ok=True)
     with cf.ThreadPoolExecutor(max_workers=len(SOURCES)) as ex:
@@ -51,6 +67,8 @@ def build(verbose: bool = False) -> str:
     if _stale(LIB, objs):
         subprocess.run([NVCC, *ARCH, "-shared", "-o", LIB, *objs, "-cudart", "static"],
                        check=True)
+    with cf.ThreadPoolExecutor(max_workers=3) as ex:
+        list(ex.map(_compat, (1, 2, 3)))
     return LIB
 
 

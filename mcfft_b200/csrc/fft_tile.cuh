@@ -1,0 +1,521 @@
+// fft_tile.cuh -- warp-specialised, TMA-fed FFT pass kernel (sm_100a).
+//
+// One persistent CTA per SM processes tiles of C columns x L points
+// (L = 16^a * R, R in {1,2,4,8}) of one pass of a batched C2C FFT:
+//
+//   producer warp   TMA bulk-tensor load of tile i+2 into staging buffer
+//                   b = i % 2 once tile i's output has left it; TMA bulk-
+//                   tensor store of tile i's output from the same buffer
+//   consumer warps  prologue: staging -> registers -> [radix-R stage in
+//                   FP32] -> FP16 -> tcgen05 A operand (K-major, 64-byte
+//                   swizzle); per radix-16 stage: one thread issues the
+//                   tcgen05.mma (D = A * DFT16, FP32 in TMEM), every warp
+//                   drains its TMEM sub-partition with tcgen05.ld, applies
+//                   twiddle and scale, and stores into the next stage's A
+//                   rows -- or, after the last stage, into the staging
+//                   buffer in natural order for the TMA store.
+//
+// All addressing comes from host-built tables (layout.cpp): per prologue
+// item a load/store base, per A row and stage a destination base; the
+// per-element offsets are XOR constants passed as kernel parameters, so a
+// stored element costs one XOR and one st.shared.  The layouts are chosen
+// on the host to be free of shared-memory bank conflicts.
+//
+// Synchronisation: mbarriers for TMA completion (full[b]), for "output
+// staged" (outrdy[b]) and for MMA completion (dfull, via tcgen05.commit);
+// named barrier 1 among consumer warps.  Every wait is bounded; on timeout
+// the kernel records kStatusTimeout in the status word and winds down.
+#pragma once
+#include <cuda.h>
+#include <cstdint>
+#include <cuda_fp16.h>
+
+#include "fft_pass.cuh"
+#include "mcfft_internal.h"
+#include "sm100_ptx.cuh"
+
+namespace mcfft {
+
+constexpr int kMaxStages = 4;
+
+struct alignas(64) TileArgs {
+  CUtensorMap tmap_in;
+  CUtensorMap tmap_out;
+  int32_t in_cmul[5], in_omul[5], out_cmul[5], out_omul[5];
+  int32_t in_ndims, out_ndims;
+  int64_t col_blocks, ntiles;
+  uint32_t in_tile_bytes;
+  const uint2* item_tab;   // per prologue item: {lds_base>>2 | sts_base>>2 << 16, tail twiddle row}
+  const uint32_t* epi_tab; // [stage][row]: dst_base>>2 | aux << 16
+  uint32_t lofs[8];        // XOR offsets of an item's loads
+  uint32_t sofs[32];       // XOR offsets of an item's stores
+  uint32_t kofs[kMaxStages][16];
+  const float2* tw;        // stage twiddles (scaled by 1/16), stages concatenated, [R'][k]
+  const float2* tail_tw;   // radix-R twiddles (scaled by 1/R), [v][k]
+  const uint4* bmat;       // DFT-16 embedding (hi), 64B-swizzled K-major, 2 KB
+  const uint4* bmat_lo;    // split form: low part
+  const float2* post_a;    // four-step: W_N^e low table, e in [0, 2^post_shift)
+  const float2* post_b;    // four-step: W_N^(e << post_shift) high table
+  uint64_t post_mask;      // N - 1
+  uint32_t post_shift;
+  float out_scale;
+  int inverse;
+  int split_in_f16;
+  int* status;
+};
+
+namespace tile {
+
+__device__ __forceinline__ void named_bar(int id, int n) {
+  asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(n) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(sm100::smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ uint4 lds128(uint32_t addr) {
+  uint4 v;
+  asm volatile("ld.shared.v4.b32 {%0,%1,%2,%3}, [%4];"
+               : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
+               : "r"(addr));
+  return v;
+}
+__device__ __forceinline__ void sts128(uint32_t addr, uint4 v) {
+  asm volatile("st.shared.v4.b32 [%0], {%1,%2,%3,%4};" ::"r"(addr), "r"(v.x), "r"(v.y), "r"(v.z),
+               "r"(v.w)
+               : "memory");
+}
+__device__ __forceinline__ void sts32(uint32_t addr, uint32_t v) {
+  asm volatile("st.shared.b32 [%0], %1;" ::"r"(addr), "r"(v) : "memory");
+}
+__device__ __forceinline__ void sts64(uint32_t addr, float2 v) {
+  asm volatile("st.shared.v2.f32 [%0], {%1,%2};" ::"r"(addr), "f"(v.x), "f"(v.y) : "memory");
+}
+
+// TMA bulk-tensor load / store of one tile; coordinates from the recipe.
+__device__ __forceinline__ void tma_load(const CUtensorMap* map, int nd, const int32_t* crd,
+                                         uint32_t dst, uint64_t* bar) {
+  const uint64_t m = reinterpret_cast<uint64_t>(map);
+  const uint32_t mb = sm100::smem_u32(bar);
+  if (nd == 3)
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(dst),
+        "l"(m), "r"(crd[0]), "r"(crd[1]), "r"(crd[2]), "r"(mb)
+        : "memory");
+  else if (nd == 4)
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(dst),
+        "l"(m), "r"(crd[0]), "r"(crd[1]), "r"(crd[2]), "r"(crd[3]), "r"(mb)
+        : "memory");
+  else
+    asm volatile(
+        "cp.async.bulk.tensor.5d.shared::cluster.global.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%2, %3, %4, %5, %6}], [%7];" ::"r"(dst),
+        "l"(m), "r"(crd[0]), "r"(crd[1]), "r"(crd[2]), "r"(crd[3]), "r"(crd[4]), "r"(mb)
+        : "memory");
+}
+__device__ __forceinline__ void tma_store(const CUtensorMap* map, int nd, const int32_t* crd,
+                                          uint32_t src) {
+  const uint64_t m = reinterpret_cast<uint64_t>(map);
+  if (nd == 3)
+    asm volatile("cp.async.bulk.tensor.3d.global.shared::cta.bulk_group [%0, {%1, %2, %3}], [%4];" ::"l"(m),
+                 "r"(crd[0]), "r"(crd[1]), "r"(crd[2]), "r"(src)
+                 : "memory");
+  else if (nd == 4)
+    asm volatile("cp.async.bulk.tensor.4d.global.shared::cta.bulk_group [%0, {%1, %2, %3, %4}], [%5];" ::"l"(m),
+                 "r"(crd[0]), "r"(crd[1]), "r"(crd[2]), "r"(crd[3]), "r"(src)
+                 : "memory");
+  else
+    asm volatile(
+        "cp.async.bulk.tensor.5d.global.shared::cta.bulk_group [%0, {%1, %2, %3, %4, %5}], [%6];" ::"l"(m),
+        "r"(crd[0]), "r"(crd[1]), "r"(crd[2]), "r"(crd[3]), "r"(crd[4]), "r"(src)
+        : "memory");
+  asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+}
+__device__ __forceinline__ void tma_store_wait_read() {
+  asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+}
+__device__ __forceinline__ void tma_store_wait_all() {
+  asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
+}
+
+// K-major, 64-byte-swizzled shared-memory matrix descriptor (8-row atoms of
+// 512 bytes; `sbo` = 512 between atoms).
+__device__ __forceinline__ uint64_t sdesc_sw64(uint32_t saddr) {
+  uint64_t d = 0;
+  d |= static_cast<uint64_t>((saddr & 0x3FFFFu) >> 4);
+  d |= static_cast<uint64_t>(1) << 16;                 // LBO (unused for swizzled K-major)
+  d |= static_cast<uint64_t>(512u >> 4) << 32;         // SBO
+  d |= static_cast<uint64_t>(1) << 46;                 // sm_100 descriptor version
+  d |= static_cast<uint64_t>(4) << 61;                 // SWIZZLE_64B
+  return d;
+}
+
+__device__ __forceinline__ void tile_coords(const int32_t* cm, const int32_t* om, int64_t cb,
+                                            int64_t outer, int32_t* crd) {
+#pragma unroll
+  for (int d = 0; d < 5; ++d) crd[d] = (int32_t)(cb * cm[d] + outer * om[d]);
+}
+
+}  // namespace tile
+
+template <int L, int R, int C, int NCW>
+struct TileShape {
+  static constexpr int NV = L / 16;
+  static constexpr int NROWS = NV * C;
+  static constexpr int NMT = NROWS / 128;
+  static constexpr int NST = ilog2c(L / R) / 4;
+  static constexpr int NCT = NCW * 32;
+  static constexpr int NT = NCT + 32;
+  static constexpr int TMEM_COLS = pow2ceil(NMT * 32 < 32 ? 32 : NMT * 32);
+  static constexpr int ITEMS = R == 1 ? L * C / 16 : L * C / (4 * R);
+  static_assert(NROWS % 128 == 0, "tile must hold a multiple of 128 vectors");
+  static_assert(NMT * 32 <= 512, "tile exceeds tensor memory");
+  static_assert(NST >= 1 && NST <= kMaxStages, "stage count");
+};
+
+// Plain FP16 form.  Staging holds FP16 complex (4 bytes) in and out.
+// Stage twiddle entries of all non-last stages: sum of L / P_s.
+template <int L, int R>
+constexpr int stage_tw_entries() {
+  int n = 0, Ls = L / R, nst = ilog2c(L / R) / 4;
+  for (int s = 0; s < nst - 1; ++s) { n += Ls; Ls >>= 4; }
+  return n;
+}
+
+template <int L, int R, int C, bool POSTTW, int NCW>
+struct TileF16 {
+  using S = TileShape<L, R, C, NCW>;
+  static constexpr int STAGE_BYTES = L * C * 4;
+  static constexpr int A_BYTES = S::NROWS * 64;
+  // Twiddle tables that are constant for the whole launch live in shared
+  // memory when they are small (radix-R table always, stage tables up to
+  // 2048 entries); larger stage tables are read through L1.
+  static constexpr int TW_ENTRIES = stage_tw_entries<L, R>();
+  static constexpr bool TW_SMEM = TW_ENTRIES <= 2048;
+  static constexpr int TAIL_BYTES = R > 1 ? L * 8 : 0;
+  static constexpr int TWS_BYTES = TW_SMEM ? TW_ENTRIES * 8 : 0;
+  static constexpr int OFF_S0 = 0;
+  static constexpr int OFF_S1 = STAGE_BYTES;
+  static constexpr int OFF_A = 2 * STAGE_BYTES;
+  static constexpr int OFF_B = OFF_A + A_BYTES;
+  static constexpr int OFF_TAIL = OFF_B + 2048;
+  static constexpr int OFF_TWS = OFF_TAIL + TAIL_BYTES;
+  static constexpr int OFF_BAR = OFF_TWS + TWS_BYTES;
+  static constexpr int SMEM_BYTES = OFF_BAR + 128 + 1024;  // + alignment slack
+  static_assert(SMEM_BYTES <= 232448, "shared memory budget");
+};
+
+__device__ __forceinline__ float2 lds64f(uint32_t addr) {
+  float2 v;
+  asm volatile("ld.shared.v2.f32 {%0,%1}, [%2];" : "=f"(v.x), "=f"(v.y) : "r"(addr));
+  return v;
+}
+__device__ __forceinline__ float4 lds128f(uint32_t addr) {
+  float4 v;
+  asm volatile("ld.shared.v4.f32 {%0,%1,%2,%3}, [%4];" : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w) : "r"(addr));
+  return v;
+}
+
+// W_N^e from the two-level table: lo[e & (2^sh - 1)] * hi[e >> sh].
+__device__ __forceinline__ float2 twiddle2(const float2* lo, const float2* hi, uint64_t e, uint32_t sh) {
+  return cmulf(__ldg(lo + (e & ((1ull << sh) - 1))), __ldg(hi + (e >> sh)));
+}
+
+template <int L, int R, int C, bool POSTTW, int NCW>
+__global__ void __launch_bounds__(NCW * 32 + 32, NCW <= 8 ? 2 : 1) fft_tile_f16(const __grid_constant__ TileArgs a) {
+  using S = TileShape<L, R, C, NCW>;
+  using T = TileF16<L, R, C, POSTTW, NCW>;
+  constexpr int NCT = S::NCT;
+  constexpr int NIT_P = (S::ITEMS + NCT - 1) / NCT;  // prologue items per consumer thread
+  constexpr int NIT_E = S::NMT * 4 / NCW;            // 32-row blocks per warp per stage
+  static_assert(S::NMT * 4 % NCW == 0, "row blocks per warp");
+  extern __shared__ uint8_t smem_raw[];
+  // 1024-byte alignment for the swizzled TMA boxes and the UMMA atoms.
+  const uint32_t raw_u = sm100::smem_u32(smem_raw);
+  const uint32_t base_u = (raw_u + 1023u) & ~1023u;
+  uint8_t* smem = smem_raw + (base_u - raw_u);
+  const uint32_t sS0 = base_u + T::OFF_S0, sS1 = base_u + T::OFF_S1;
+  const uint32_t sA = base_u + T::OFF_A;
+  const uint32_t sB = base_u + T::OFF_B;
+  const uint32_t sTail = base_u + T::OFF_TAIL;
+  const uint32_t sTws = base_u + T::OFF_TWS;
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + T::OFF_BAR);      // [2]
+  uint64_t* outrdy = full + 2;                                          // [2]
+  uint64_t* dfull = full + 4;                                           // [1]
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(full + 5);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(full + 6);
+
+  const int tid = threadIdx.x;
+  const int warp = tid >> 5, lane = tid & 31;
+  const bool producer = warp == NCW;
+
+  if (producer) {
+    if (lane == 0) {
+      sm100::mbar_init(&full[0], 1);
+      sm100::mbar_init(&full[1], 1);
+      sm100::mbar_init(&outrdy[0], 1);
+      sm100::mbar_init(&outrdy[1], 1);
+      sm100::mbar_init(dfull, 1);
+      *abort_flag = 0;
+      sm100::fence_mbar_init();
+    }
+    __syncwarp();
+    sm100::tmem_alloc(tmem_slot, S::TMEM_COLS);
+    sm100::tmem_relinquish();
+  } else {
+    for (int i = tid; i < 128; i += NCT)
+      *reinterpret_cast<uint4*>(smem + T::OFF_B + 16 * i) = __ldg(a.bmat + i);
+    if constexpr (R > 1) {
+      for (int i = tid; i < L / 2; i += NCT)
+        *reinterpret_cast<float4*>(smem + T::OFF_TAIL + 16 * i) =
+            __ldg(reinterpret_cast<const float4*>(a.tail_tw) + i);
+    }
+    if constexpr (T::TW_SMEM && T::TW_ENTRIES > 0) {
+      for (int i = tid; i < T::TW_ENTRIES / 2; i += NCT)
+        *reinterpret_cast<float4*>(smem + T::OFF_TWS + 16 * i) =
+            __ldg(reinterpret_cast<const float4*>(a.tw) + i);
+    }
+  }
+  sm100::fence_proxy_async_smem();
+  sm100::tc_fence_before();
+  __syncthreads();
+  sm100::tc_fence_after();
+  const uint32_t tmem_base = *tmem_slot;
+
+  if (producer) {
+    // ------------------------------------------------------------- producer
+    if (lane == 0) {
+      bool pending[2] = {false, false};
+      uint32_t pend_par[2] = {0u, 0u};
+      for (int j = 0; j < 2; ++j) {
+        const int64_t t = blockIdx.x + (int64_t)j * gridDim.x;
+        if (t < a.ntiles) {
+          int32_t crd[5];
+          tile::tile_coords(a.in_cmul, a.in_omul, t % a.col_blocks, t / a.col_blocks, crd);
+          sm100::mbar_arrive_expect_tx(&full[j], a.in_tile_bytes);
+          tile::tma_load(&a.tmap_in, a.in_ndims, crd, j ? sS1 : sS0, &full[j]);
+          pending[j] = true;
+          pend_par[j] = 0;
+        }
+      }
+      int i = 0;
+      for (int64_t t = blockIdx.x; t < a.ntiles; t += gridDim.x, ++i) {
+        const int b = i & 1;
+        const uint32_t sb = b ? sS1 : sS0;
+        if (!sm100::mbar_wait_bounded(&outrdy[b], (i >> 1) & 1, kWaitLimit) || *abort_flag) {
+          *abort_flag = 1;
+          break;
+        }
+        pending[b] = false;  // the consumers waited on full[b] for this tile
+        int32_t crd[5];
+        tile::tile_coords(a.out_cmul, a.out_omul, t % a.col_blocks, t / a.col_blocks, crd);
+        tile::tma_store(&a.tmap_out, a.out_ndims, crd, sb);
+        tile::tma_store_wait_read();
+        const int64_t t2 = t + 2 * (int64_t)gridDim.x;
+        if (t2 < a.ntiles) {
+          tile::tile_coords(a.in_cmul, a.in_omul, t2 % a.col_blocks, t2 / a.col_blocks, crd);
+          sm100::mbar_arrive_expect_tx(&full[b], a.in_tile_bytes);
+          tile::tma_load(&a.tmap_in, a.in_ndims, crd, sb, &full[b]);
+          pending[b] = true;
+          pend_par[b] = ((i + 2) >> 1) & 1;
+        }
+      }
+      tile::tma_store_wait_all();
+      // Loads issued but never consumed (abort path) must land before the
+      // CTA's shared memory is released.
+      for (int b = 0; b < 2; ++b)
+        if (pending[b]) sm100::mbar_wait_bounded(&full[b], pend_par[b], kWaitLimit);
+    }
+    __syncwarp();
+  } else {
+    // ------------------------------------------------------------ consumers
+    const int ctid = tid;  // 0 .. NCT-1
+    const int sp = warp & 3;
+    constexpr uint32_t IDESC = sm100::idesc_f16_f32(128, 32);
+    uint32_t dphase = 0;
+    const float tsgn = a.inverse ? 1.f : -1.f;
+
+    // The tables are the same for every tile: keep this thread's entries in
+    // registers for the whole launch.
+    uint2 ient[NIT_P];
+#pragma unroll
+    for (int j = 0; j < NIT_P; ++j) {
+      const int it = ctid + j * NCT;
+      ient[j] = it < S::ITEMS ? __ldg(a.item_tab + it) : make_uint2(0u, 0u);
+    }
+    uint32_t eent[S::NST][NIT_E];
+#pragma unroll
+    for (int s = 0; s < S::NST; ++s)
+#pragma unroll
+      for (int j = 0; j < NIT_E; ++j) {
+        const uint32_t m = (warp >> 2) + j * (NCW / 4);
+        eent[s][j] = __ldg(a.epi_tab + s * S::NROWS + m * 128 + sp * 32 + lane);
+      }
+
+    int i = 0;
+    for (int64_t t = blockIdx.x; t < a.ntiles; t += gridDim.x, ++i) {
+      const int b = i & 1;
+      const uint32_t sb = b ? sS1 : sS0;
+      const int64_t cb = t % a.col_blocks;
+      if (!sm100::mbar_wait_bounded(&full[b], (i >> 1) & 1, kWaitLimit)) *abort_flag = 1;
+      if (*abort_flag) break;
+
+      // ---------------------------------------------------------- prologue
+      // Offsets are XOR-linear relative to their buffer: XOR first, then add
+      // the buffer base.
+#pragma unroll
+      for (int j = 0; j < NIT_P; ++j) {
+        if (S::ITEMS % NCT != 0 && ctid + j * NCT >= S::ITEMS) break;
+        const uint2 e = ient[j];
+        const uint32_t lb = (e.x & 0xFFFFu) << 2;
+        const uint32_t st = (e.x >> 16) << 2;
+        if constexpr (R == 1) {
+          const uint4 q0 = tile::lds128(sb + (lb ^ a.lofs[0]));
+          const uint4 q1 = tile::lds128(sb + (lb ^ a.lofs[1]));
+          const uint4 q2 = tile::lds128(sb + (lb ^ a.lofs[2]));
+          const uint4 q3 = tile::lds128(sb + (lb ^ a.lofs[3]));
+          tile::sts128(sA + (st ^ a.sofs[0]), make_uint4(q0.x, q1.x, q2.x, q3.x));
+          tile::sts128(sA + (st ^ a.sofs[1]), make_uint4(q0.y, q1.y, q2.y, q3.y));
+          tile::sts128(sA + (st ^ a.sofs[2]), make_uint4(q0.z, q1.z, q2.z, q3.z));
+          tile::sts128(sA + (st ^ a.sofs[3]), make_uint4(q0.w, q1.w, q2.w, q3.w));
+        } else {
+          uint4 q[R];
+#pragma unroll
+          for (int n = 0; n < R; ++n) q[n] = tile::lds128(sb + (lb ^ a.lofs[n]));
+          // item word 1: tail twiddle row of sub-vector 0; bit 31 set for
+          // column items (all four sub-vectors share the row)
+          const uint32_t trow = e.y & 0x7FFFFFFFu;
+          const bool colitem = (e.y >> 31) != 0;
+#pragma unroll
+          for (int jj = 0; jj < 4; ++jj) {
+            float2 x[R];
+#pragma unroll
+            for (int n = 0; n < R; ++n) {
+              const uint32_t w = jj == 0 ? q[n].x : jj == 1 ? q[n].y : jj == 2 ? q[n].z : q[n].w;
+              x[n] = sm100::unpack_half2(w);
+            }
+            small_dft<R>(x, tsgn);
+            const uint32_t vr = colitem ? trow : trow + jj;
+            const uint32_t twa = sTail + vr * (R * 8);
+#pragma unroll
+            for (int k2 = 0; k2 < R / 2; ++k2) {
+              const float4 tw4 = lds128f(twa + 16 * k2);
+              const float2 y0 = cmulf(x[2 * k2], make_float2(tw4.x, tw4.y));
+              const float2 y1 = cmulf(x[2 * k2 + 1], make_float2(tw4.z, tw4.w));
+              tile::sts32(sA + (st ^ a.sofs[jj * R + 2 * k2]), sm100::pack_half2(y0.x, y0.y));
+              tile::sts32(sA + (st ^ a.sofs[jj * R + 2 * k2 + 1]), sm100::pack_half2(y1.x, y1.y));
+            }
+          }
+        }
+      }
+      sm100::fence_proxy_async_smem();
+      sm100::tc_fence_before();
+      tile::named_bar(1, NCT);
+      sm100::tc_fence_after();
+
+      // ------------------------------------------------------------ stages
+#pragma unroll
+      for (int s = 0; s < S::NST; ++s) {
+        constexpr bool dummy = false;
+        (void)dummy;
+        if (ctid == 0) {
+#pragma unroll 1
+          for (int m = 0; m < S::NMT; ++m) {
+#pragma unroll
+            for (int ks = 0; ks < 2; ++ks)
+              sm100::umma_f16(tmem_base + 32u * m, tile::sdesc_sw64(sA + m * 8192u + ks * 32u),
+                              tile::sdesc_sw64(sB + ks * 32u), IDESC, ks);
+          }
+          sm100::umma_commit(dfull);
+        }
+        const bool last = s == S::NST - 1;
+        const uint32_t stw_off = stage_tw_offset<L, R>(s);
+        // Prefetch the first block's twiddles while the MMAs run (global
+        // stage tables only; shared-memory tables are read in the loop).
+        float4 wpre[8];
+        if (!last && !T::TW_SMEM) {
+          const float4* t4 = reinterpret_cast<const float4*>(a.tw + stw_off + (eent[s][0] >> 16) * 16);
+#pragma unroll
+          for (int k2 = 0; k2 < 8; ++k2) wpre[k2] = __ldg(t4 + k2);
+        }
+        if (!sm100::mbar_wait_bounded(dfull, dphase, kWaitLimit)) *abort_flag = 1;
+        dphase ^= 1u;
+        sm100::tc_fence_after();
+#pragma unroll
+        for (int j = 0; j < NIT_E; ++j) {
+          const uint32_t m = (warp >> 2) + j * (NCW / 4);
+          const uint32_t e = eent[s][j];
+          const uint32_t aux = e >> 16;
+          const uint32_t dst = (e & 0xFFFFu) << 2;
+          uint32_t d[32];
+          sm100::tmem_ld32(tmem_base + ((uint32_t)(32 * sp) << 16) + 32u * m, d);
+          if (!last) {
+            float4 w[8];
+            if (T::TW_SMEM) {
+#pragma unroll
+              for (int k2 = 0; k2 < 8; ++k2) w[k2] = lds128f(sTws + (stw_off + aux * 16) * 8 + 16 * k2);
+            } else if (j == 0) {
+#pragma unroll
+              for (int k2 = 0; k2 < 8; ++k2) w[k2] = wpre[k2];
+            } else {
+              const float4* t4 = reinterpret_cast<const float4*>(a.tw + stw_off + aux * 16);
+#pragma unroll
+              for (int k2 = 0; k2 < 8; ++k2) w[k2] = __ldg(t4 + k2);
+            }
+            sm100::tmem_wait_ld();
+#pragma unroll
+            for (int k = 0; k < 16; ++k) {
+              const float4 ww = w[k >> 1];
+              const float2 tw = (k & 1) ? make_float2(ww.z, ww.w) : make_float2(ww.x, ww.y);
+              const float2 y =
+                  cmulf(make_float2(__uint_as_float(d[2 * k]), __uint_as_float(d[2 * k + 1])), tw);
+              tile::sts32(sA + (dst ^ a.kofs[s][k]), sm100::pack_half2(y.x, y.y));
+            }
+          } else if (POSTTW) {
+            // Four-step twiddle W_N^((v + NV k) g): w_0 = W_N^(v g), then
+            // w_(k+1) = w_k * W_N^(NV g) (FP32 recurrence, 15 steps, far
+            // below the FP16 output rounding).
+            const uint32_t v = aux / C, c = aux % C;
+            const uint64_t g = (uint64_t)(cb * C + c);
+            const uint64_t e0 = ((uint64_t)v * g) & a.post_mask;
+            const uint64_t es = ((uint64_t)S::NV * g) & a.post_mask;
+            float2 wk = twiddle2(a.post_a, a.post_b, e0, a.post_shift);
+            const float2 ws = twiddle2(a.post_a, a.post_b, es, a.post_shift);
+            wk.x *= a.out_scale;
+            wk.y *= a.out_scale;
+            sm100::tmem_wait_ld();
+#pragma unroll
+            for (int k = 0; k < 16; ++k) {
+              const float2 y =
+                  cmulf(make_float2(__uint_as_float(d[2 * k]), __uint_as_float(d[2 * k + 1])), wk);
+              tile::sts32(sb + (dst ^ a.kofs[s][k]), sm100::pack_half2(y.x, y.y));
+              wk = cmulf(wk, ws);
+            }
+          } else {
+            sm100::tmem_wait_ld();
+#pragma unroll
+            for (int k = 0; k < 16; ++k) {
+              const float yr = __uint_as_float(d[2 * k]) * a.out_scale;
+              const float yi = __uint_as_float(d[2 * k + 1]) * a.out_scale;
+              tile::sts32(sb + (dst ^ a.kofs[s][k]), sm100::pack_half2(yr, yi));
+            }
+          }
+        }
+        sm100::fence_proxy_async_smem();
+        sm100::tc_fence_before();
+        tile::named_bar(1, NCT);
+        sm100::tc_fence_after();
+        if (*abort_flag) break;
+      }
+      if (*abort_flag) break;
+      if (ctid == 0) tile::mbar_arrive(&outrdy[b]);
+    }
+  }
+  __syncthreads();
+  if (tid == 0 && *abort_flag && a.status) atomicExch(a.status, kStatusTimeout);
+  if (producer) sm100::tmem_dealloc(tmem_base, S::TMEM_COLS);
+}
+
+}  // namespace mcfft

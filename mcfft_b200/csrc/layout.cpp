@@ -1,0 +1,585 @@
+// layout.cpp -- see layout.h.
+#include "layout.h"
+
+#include <algorithm>
+#include <cstdio>
+#include <functional>
+#include <map>
+#include <set>
+#include <sstream>
+
+namespace mcfft {
+namespace layout {
+
+namespace {
+
+int ilog2(int64_t x) {
+  int r = 0;
+  while ((int64_t(1) << r) < x) ++r;
+  return r;
+}
+
+int swz_for(int row_bytes) {
+  return row_bytes >= 128 ? 7 : row_bytes == 64 ? 3 : row_bytes == 32 ? 1 : 0;
+}
+
+// Bit ids: v bit j -> j, c bit j -> 64 + j.
+constexpr int kC = 64;
+
+struct RowMap {
+  std::vector<int> src;  // r bit i <- source bit id src[i]
+  std::vector<uint32_t> tv, tc;  // contributions of v and of c (disjoint bits)
+  uint32_t apply(uint32_t v, uint32_t c) const { return tv[v] | tc[c]; }
+};
+
+RowMap make_rowmap(const std::vector<int>& low, int b, int g) {
+  RowMap m;
+  std::set<int> used(low.begin(), low.end());
+  m.src = low;
+  for (int j = 0; j < g; ++j)
+    if (!used.count(kC + j)) m.src.push_back(kC + j);
+  for (int j = 0; j < b; ++j)
+    if (!used.count(j)) m.src.push_back(j);
+  m.tv.assign((size_t)1 << b, 0);
+  m.tc.assign((size_t)1 << g, 0);
+  for (size_t i = 0; i < m.src.size(); ++i) {
+    const int s = m.src[i];
+    if (s >= kC) {
+      for (uint32_t c = 0; c < m.tc.size(); ++c) m.tc[c] |= ((c >> (s - kC)) & 1u) << i;
+    } else if (s < b) {
+      for (uint32_t v = 0; v < m.tv.size(); ++v) m.tv[v] |= ((v >> s) & 1u) << i;
+    }
+  }
+  return m;
+}
+
+// ---- bank-conflict model --------------------------------------------------
+// Wavefronts of one warp-wide shared-memory access.  16-byte accesses are
+// served per quarter-warp (8 lanes); within a group, lanes touching the same
+// 16-byte bank group at different addresses serialise.  4-byte accesses:
+// all 32 lanes; distinct words in one bank serialise.
+double wavefronts(const std::vector<uint32_t>& addr, int bytes) {
+  if (bytes == 16) {
+    double w = 0;
+    for (size_t p = 0; p < addr.size(); p += 8) {
+      uint32_t seen[8][8];
+      int cnt[8] = {0};
+      int m = 0;
+      for (size_t i = p; i < std::min(addr.size(), p + 8); ++i) {
+        const int g = (addr[i] >> 4) & 7;
+        const uint32_t a = addr[i] >> 4;
+        bool dup = false;
+        for (int k = 0; k < cnt[g]; ++k) dup |= seen[g][k] == a;
+        if (!dup) seen[g][cnt[g]++] = a;
+        m = std::max(m, cnt[g]);
+      }
+      w += m;
+    }
+    return w;
+  }
+  uint32_t seen[32][32];
+  int cnt[32] = {0};
+  int m = 0;
+  for (uint32_t a : addr) {
+    const int g = (a >> 2) & 31;
+    const uint32_t wd = a >> 2;
+    bool dup = false;
+    for (int k = 0; k < cnt[g]; ++k) dup |= seen[g][k] == wd;
+    if (!dup && cnt[g] < 32) seen[g][cnt[g]++] = wd;
+    m = std::max(m, cnt[g]);
+  }
+  return m;
+}
+double ideal_wavefronts(size_t lanes, int bytes) {
+  return bytes == 16 ? (double)((lanes + 7) / 8) : 1.0;
+}
+
+}  // namespace
+
+uint32_t Staging::offset(uint32_t pos, uint32_t c) const {
+  uint32_t raw;
+  if (kind == ROW)
+    raw = ((pos / E) * C + c) * row_bytes + (pos % E) * elem;
+  else
+    raw = ((c / E) * L + pos) * row_bytes + (c % E) * elem;
+  return raw ^ (((raw >> 7) & swz) << 4);
+}
+
+Staging make_staging(Kind kind, int L, int C, int elem, int64_t sp, int64_t sc, int64_t so,
+                     int64_t ncols, int64_t nouter) {
+  Staging s;
+  s.kind = kind;
+  s.L = L;
+  s.C = C;
+  s.elem = elem;
+  const int per_row = 128 / elem;
+  if (kind == ROW) {
+    s.E = std::min(L, per_row);
+    s.row_bytes = s.E * elem;
+    s.swz = swz_for(s.row_bytes);
+    // dims: point-low (E), column, point-high (L/E), outer
+    s.ndims = 4;
+    s.gdim[0] = (uint64_t)s.E;            s.box[0] = (uint32_t)s.E;
+    s.gdim[1] = (uint64_t)ncols;          s.box[1] = (uint32_t)C;  s.gstride_bytes[1] = (uint64_t)sc * elem;
+    s.gdim[2] = (uint64_t)(L / s.E);      s.box[2] = (uint32_t)(L / s.E); s.gstride_bytes[2] = (uint64_t)s.E * sp * elem;
+    s.gdim[3] = (uint64_t)nouter;         s.box[3] = 1;            s.gstride_bytes[3] = (uint64_t)so * elem;
+    s.cmul[1] = C;
+    s.omul[3] = 1;
+    if (nouter <= 1) s.ndims = 3;
+  } else {
+    s.E = std::min(C, per_row);
+    s.row_bytes = s.E * elem;
+    s.swz = swz_for(s.row_bytes);
+    const int plo = std::min(L, 256), phi = L / plo;
+    // dims: column-low (E), point-low, point-high, column-high, outer
+    s.ndims = 5;
+    s.gdim[0] = (uint64_t)s.E;             s.box[0] = (uint32_t)s.E;
+    s.gdim[1] = (uint64_t)plo;             s.box[1] = (uint32_t)plo; s.gstride_bytes[1] = (uint64_t)sp * elem;
+    s.gdim[2] = (uint64_t)phi;             s.box[2] = (uint32_t)phi; s.gstride_bytes[2] = (uint64_t)plo * sp * elem;
+    s.gdim[3] = (uint64_t)(ncols / s.E);   s.box[3] = (uint32_t)(C / s.E); s.gstride_bytes[3] = (uint64_t)s.E * elem;
+    s.gdim[4] = (uint64_t)nouter;          s.box[4] = 1;             s.gstride_bytes[4] = (uint64_t)so * elem;
+    s.cmul[3] = C / s.E;
+    s.omul[4] = 1;
+    if (nouter <= 1) s.ndims = 4;
+  }
+  return s;
+}
+
+namespace {
+
+struct Ctx {
+  PassLayout* pl;
+  int b, g, rb;
+};
+
+// Epilogue of stage s with row maps m[s], m[s+1] (or the output staging for
+// the last stage).  Fills tables if `fill`; returns excess wavefronts.
+double eval_epilogue(const Ctx& x, const std::vector<RowMap>& m, int s, bool fill,
+                     std::vector<uint32_t>* tab, std::vector<uint32_t>* kofs, bool* linear) {
+  PassLayout& p = *x.pl;
+  const uint32_t P = (uint32_t)p.R << (4 * s);
+  const bool last = s == p.NST - 1;
+  // row -> (v, c)
+  std::vector<uint32_t> rv(p.NROWS), rc(p.NROWS);
+  for (int v = 0; v < p.NV; ++v)
+    for (int c = 0; c < p.C; ++c) {
+      uint32_t r = m[s].apply(v, c);
+      rv[r] = v;
+      rc[r] = c;
+    }
+  std::vector<uint32_t> ofs(16);
+  double w = 0, ideal = 0;
+  std::vector<uint32_t> base(p.NROWS);
+  for (int r = 0; r < p.NROWS; ++r) {
+    const uint32_t v = rv[r], c = rc[r];
+    for (int k = 0; k < 16; ++k) {
+      uint32_t d;
+      if (!last) {
+        const uint32_t K = v % P, Rp = v / P;
+        const uint32_t pos1 = K + P * (k + 16 * Rp);
+        const uint32_t n1 = pos1 / p.NV, v1 = pos1 % p.NV;
+        d = a_offset(m[s + 1].apply(v1, c), n1);
+      } else {
+        d = p.out.offset(v + p.NV * k, c);
+      }
+      if (k == 0) base[r] = d;
+      const uint32_t o = d ^ base[r];
+      if (r == 0) ofs[k] = o;
+      else if (ofs[k] != o && linear) *linear = false;
+    }
+  }
+  // conflicts: warps = 32 consecutive rows, one store per k
+  const int bytes = last ? p.out.elem : 4;
+  const int wstep = fill ? 32 : 32 * std::max(1, p.NROWS / 256);  // sample warps while searching
+  for (int r0 = 0; r0 < p.NROWS; r0 += wstep) {
+    for (int k = 0; k < 16; ++k) {
+      std::vector<uint32_t> a;
+      for (int l = 0; l < 32 && r0 + l < p.NROWS; ++l) a.push_back(base[r0 + l] ^ ofs[k]);
+      if (bytes == 8) {
+        // 64-bit stores: two half-warp phases
+        std::vector<uint32_t> lo(a.begin(), a.begin() + std::min<size_t>(16, a.size()));
+        std::vector<uint32_t> hi(a.begin() + std::min<size_t>(16, a.size()), a.end());
+        auto w64 = [](const std::vector<uint32_t>& aa) {
+          std::map<int, std::set<uint32_t>> gg;
+          for (uint32_t q : aa) { gg[(q >> 2) & 31].insert(q >> 3); gg[((q >> 2) + 1) & 31].insert(q >> 3); }
+          size_t mm = 0;
+          for (auto& kv : gg) mm = std::max(mm, kv.second.size());
+          return (double)mm;
+        };
+        w += w64(lo) + w64(hi);
+        ideal += 2;
+      } else {
+        w += wavefronts(a, 4);
+        ideal += 1;
+      }
+    }
+  }
+  if (fill) {
+    for (int r = 0; r < p.NROWS; ++r) {
+      const uint32_t v = rv[r], c = rc[r];
+      uint32_t aux = last ? v * p.C + c : v / P;
+      (*tab)[(size_t)s * p.NROWS + r] = (base[r] >> 2) | (aux << 16);
+    }
+    for (int k = 0; k < 16; ++k) (*kofs)[(size_t)s * 16 + k] = ofs[k];
+  }
+  return w / ideal - 1.0;
+}
+
+// Prologue: items and their lane order.  `lanebits` lists the item-index
+// bits that vary fastest (the lanes of a warp), as ids into the item
+// coordinate bits.  Returns excess wavefronts; fills tables if `fill`.
+struct ItemSpace {
+  // coordinate fields of an item: (name, nbits)
+  std::vector<std::pair<char, int>> fields;
+};
+
+double eval_prologue(const Ctx& x, const RowMap& m0, const std::vector<int>& order, bool fill,
+                     bool* linear) {
+  PassLayout& p = *x.pl;
+  // item coordinate bits: ROW R=1: c(g), w(b-2), q(2); COL R=1: v(b), cg(g-2), q(2)
+  // ROW R>1: c(g), w(log2(NVR)-2); COL R>1: vr(log2 NVR), cg(g-2)
+  const int NVR = p.L / p.R;
+  const int lnvr = ilog2(NVR);
+  std::vector<int> widths;  // field widths in order: f0, f1, f2
+  if (p.R == 1) {
+    if (p.in_kind == ROW) widths = {x.g, x.b - 2, 2};
+    else widths = {x.b, x.g - 2, 2};
+  } else {
+    if (p.in_kind == ROW) widths = {x.g, lnvr - 2, 0};
+    else widths = {lnvr, x.g - 2, 0};
+  }
+  int nbits = widths[0] + widths[1] + widths[2];
+  const int nitems = 1 << nbits;
+  // order: permutation of item-coordinate bit ids (0..nbits-1), giving item
+  // index bit i <- coordinate bit order[i]
+  auto coords = [&](uint32_t idx, uint32_t* f) {
+    uint32_t cbits = 0;
+    for (int i = 0; i < nbits; ++i) cbits |= ((idx >> i) & 1u) << order[i];
+    f[0] = cbits & ((1u << widths[0]) - 1);
+    f[1] = (cbits >> widths[0]) & ((1u << widths[1]) - 1);
+    f[2] = (cbits >> (widths[0] + widths[1])) & ((1u << widths[2]) - 1);
+  };
+  const int nl = p.R == 1 ? 4 : p.R;            // loads per item
+  const int ns = p.R == 1 ? 4 : 4 * p.R;        // stores per item
+  const int sbytes = p.R == 1 ? 16 : 4;
+  std::vector<uint32_t> lb(nitems), sb(nitems), tw(nitems);
+  std::vector<uint32_t> lofs(nl), sofs(ns);
+  std::vector<uint32_t> la((size_t)nitems * nl), sa((size_t)nitems * ns);
+  const int istep = fill ? 32 : 32 * std::max(1, nitems / 256);  // sample warps while searching
+  for (int it = 0; it < nitems; ++it) {
+    if (!fill && (it % istep) >= 32) continue;
+    uint32_t f[3];
+    coords(it, f);
+    for (int j = 0; j < nl; ++j) {
+      uint32_t pos, c;
+      if (p.R == 1) {
+        if (p.in_kind == ROW) { c = f[0]; pos = (4 * f[2] + j) * p.NV + 4 * f[1]; }
+        else { c = 4 * f[1]; pos = (4 * f[2] + j) * p.NV + f[0]; }
+      } else {
+        if (p.in_kind == ROW) { c = f[0]; pos = j * NVR + 4 * f[1]; }
+        else { c = 4 * f[1]; pos = j * NVR + f[0]; }
+      }
+      la[(size_t)it * nl + j] = p.in.offset(pos, c);
+    }
+    for (int j = 0; j < ns; ++j) {
+      uint32_t d;
+      if (p.R == 1) {
+        uint32_t v, c;
+        if (p.in_kind == ROW) { c = f[0]; v = 4 * f[1] + j; }
+        else { c = 4 * f[1] + j; v = f[0]; }
+        d = a_offset(m0.apply(v, c), 4 * f[2]);
+      } else {
+        const int jj = j / p.R, k = j % p.R;
+        uint32_t vr, c;
+        if (p.in_kind == ROW) { c = f[0]; vr = 4 * f[1] + jj; }
+        else { c = 4 * f[1] + jj; vr = f[0]; }
+        const uint32_t pos1 = k + p.R * vr;
+        d = a_offset(m0.apply(pos1 % p.NV, c), pos1 / p.NV);
+      }
+      sa[(size_t)it * ns + j] = d;
+    }
+    lb[it] = la[(size_t)it * nl];
+    sb[it] = sa[(size_t)it * ns];
+    tw[it] = p.R == 1 ? 0 : (p.in_kind == ROW ? 4 * f[1] : (f[0] | 0x80000000u));
+    if (fill) {
+      for (int j = 0; j < nl; ++j) {
+        uint32_t o = la[(size_t)it * nl + j] ^ lb[it];
+        if (it == 0) lofs[j] = o;
+        else if (o != lofs[j] && linear) *linear = false;
+      }
+      for (int j = 0; j < ns; ++j) {
+        uint32_t o = sa[(size_t)it * ns + j] ^ sb[it];
+        if (it == 0) sofs[j] = o;
+        else if (o != sofs[j] && linear) *linear = false;
+      }
+    }
+  }
+  double w = 0, ideal = 0;
+  for (int i0 = 0; i0 < nitems; i0 += istep) {
+    const int n = std::min(32, nitems - i0);
+    for (int j = 0; j < nl; ++j) {
+      std::vector<uint32_t> a;
+      for (int l = 0; l < n; ++l) a.push_back(la[(size_t)(i0 + l) * nl + j]);
+      w += wavefronts(a, 16);
+      ideal += ideal_wavefronts(a.size(), 16);
+    }
+    for (int j = 0; j < ns; ++j) {
+      std::vector<uint32_t> a;
+      for (int l = 0; l < n; ++l) a.push_back(sa[(size_t)(i0 + l) * ns + j]);
+      w += wavefronts(a, sbytes);
+      ideal += ideal_wavefronts(a.size(), sbytes);
+    }
+  }
+  if (fill) {
+    p.items = nitems;
+    p.item_loads = nl;
+    p.item_stores = ns;
+    p.item_tab.assign((size_t)nitems * 2, 0);
+    for (int it = 0; it < nitems; ++it) {
+      p.item_tab[2 * it] = (lb[it] >> 2) | ((sb[it] >> 2) << 16);
+      p.item_tab[2 * it + 1] = tw[it];
+    }
+    p.lofs = lofs;
+    p.sofs = sofs;
+  }
+  return w / ideal - 1.0;
+}
+
+}  // namespace
+
+std::string PassLayout::describe() const {
+  std::ostringstream o;
+  o << "L=" << L << " R=" << R << " C=" << C << " NST=" << NST << " in=" << (in_kind == ROW ? "row" : "col")
+    << " out=" << (out_kind == ROW ? "row" : "col") << " excess(prologue)=" << prologue_excess
+    << " excess(epilogue)=" << epilogue_excess;
+  return o.str();
+}
+
+bool build(PassLayout* pl, int L, int R, int C, Kind in_kind, Kind out_kind, int in_elem,
+           int out_elem, int64_t in_sp, int64_t in_sc, int64_t in_so, int64_t out_sp,
+           int64_t out_sc, int64_t out_so, int64_t ncols, int64_t nouter, std::string* err) {
+  PassLayout& p = *pl;
+  p = PassLayout();
+  p.L = L; p.R = R; p.C = C;
+  p.NV = L / 16;
+  p.NROWS = p.NV * C;
+  p.in_kind = in_kind; p.out_kind = out_kind;
+  int nst = 0;
+  for (int t = L / R; t > 1; t >>= 4) ++nst;
+  p.NST = nst;
+  if ((1 << (4 * nst)) * R != L || nst < 1) { *err = "L is not 16^a * R"; return false; }
+  if (C < 4 || (C & (C - 1))) { *err = "C must be a power of two >= 4"; return false; }
+  if (in_kind == COL && (ncols % std::min(C, 128 / in_elem))) { *err = "ncols"; return false; }
+  if (out_kind == COL && (ncols % std::min(C, 128 / out_elem))) { *err = "ncols"; return false; }
+  p.in = make_staging(in_kind, L, C, in_elem, in_sp, in_sc, in_so, ncols, nouter);
+  p.out = make_staging(out_kind, L, C, out_elem, out_sp, out_sc, out_so, ncols, nouter);
+  Ctx x{pl, ilog2(p.NV), ilog2(C), ilog2(R)};
+
+  // Candidate bit ids for the low row bits.
+  std::vector<int> cand;
+  for (int j = 0; j < x.g; ++j) cand.push_back(kC + j);
+  for (int j = 0; j < x.b; ++j) cand.push_back(j);
+  const int top0 = x.b - 4, top1 = x.b - 3;
+
+  // Non-last stage maps: [X0, X1, X2, T0, T1]; last: [Y0..Y4].
+  std::vector<std::vector<int>> xs, ys;
+  auto combos3 = [&](std::vector<std::vector<int>>* out, const std::vector<int>& pool) {
+    for (size_t a = 0; a < pool.size(); ++a)
+      for (size_t b = 0; b < pool.size(); ++b)
+        for (size_t c = 0; c < pool.size(); ++c)
+          if (a != b && b != c && a != c && b < c) out->push_back({pool[a], pool[b], pool[c]});
+  };
+  {
+    std::vector<int> pool;
+    for (int id : cand)
+      if (x.b < 4 || (id != top0 && id != top1)) pool.push_back(id);
+    if (pool.size() > 12) pool.resize(12);
+    combos3(&xs, pool);
+    if (xs.empty()) xs.push_back({});
+  }
+  {
+    // last-stage low bits: 5 bits from a small pool (c bits and low v bits)
+    std::vector<int> pool;
+    for (int j = 0; j < std::min(x.g, 7); ++j) pool.push_back(kC + j);
+    for (int j = 0; j < std::min(x.b, 4); ++j) pool.push_back(j);
+    std::vector<std::vector<int>> cands;
+    const int n = (int)pool.size();
+    for (int m = 0; m < (1 << n); ++m) {
+      if (__builtin_popcount(m) != 5) continue;
+      std::vector<int> y;
+      for (int i = 0; i < n; ++i)
+        if (m >> i & 1) y.push_back(pool[i]);
+      // the bit placed at r bit 0 matters for the bank: try each member first
+      for (int f = 0; f < 5; ++f) {
+        std::vector<int> yy = y;
+        std::swap(yy[0], yy[f]);
+        cands.push_back(yy);
+      }
+    }
+    ys = cands;
+    if (ys.empty()) ys.push_back({});
+  }
+
+  auto lowbits_nonlast = [&](const std::vector<int>& X) {
+    std::vector<int> low = X;
+    if (x.b >= 4) { low.push_back(top0); low.push_back(top1); }
+    return low;
+  };
+
+  // Search.  The epilogue cost of stage s depends on maps[s] and maps[s+1];
+  // non-last stages share one low-bit choice X, the last stage uses Y.
+  // Rank X by the cost of stages 0..NST-3, Y by the last stage, then try
+  // the best pairs on stage NST-2.
+  auto maps_for = [&](const std::vector<int>& X, const std::vector<int>& Y,
+                      std::vector<RowMap>* maps) {
+    maps->assign(nst, RowMap());
+    for (int s = 0; s < nst; ++s) {
+      std::vector<int> low = (s == nst - 1) ? Y : lowbits_nonlast(X);
+      std::set<int> u(low.begin(), low.end());
+      if (u.size() != low.size()) return false;
+      (*maps)[s] = make_rowmap(low, x.b, x.g);
+      if ((int)(*maps)[s].src.size() != x.b + x.g) return false;
+    }
+    return true;
+  };
+  std::vector<std::pair<double, int>> xr, yr;
+  const std::vector<int> ydef = ys[0];
+  int xzero = 0, yzero = 0;
+  for (int ix = 0; ix < (nst > 1 ? (int)xs.size() : 1) && xzero < 12; ++ix) {
+    std::vector<RowMap> maps;
+    if (!maps_for(xs[ix], ydef, &maps)) { if (nst > 2) continue; }
+    double c = 0;
+    bool lin = true;
+    if (nst > 2) {
+      for (int s = 0; s < nst - 2; ++s) c += eval_epilogue(x, maps, s, false, nullptr, nullptr, &lin);
+      if (!lin) continue;
+    }
+    xr.push_back({c, ix});
+    if (c < 1e-9) ++xzero;
+  }
+  for (int iy = 0; iy < (int)ys.size() && yzero < 24; ++iy) {
+    std::vector<RowMap> maps;
+    if (!maps_for(xs.empty() ? std::vector<int>{} : xs[0], ys[iy], &maps)) continue;
+    bool lin = true;
+    double c = eval_epilogue(x, maps, nst - 1, false, nullptr, nullptr, &lin);
+    if (!lin) continue;
+    yr.push_back({c, iy});
+    if (c < 1e-9) ++yzero;
+  }
+  std::sort(xr.begin(), xr.end());
+  std::sort(yr.begin(), yr.end());
+  struct Cand { double cost; std::vector<RowMap> maps; };
+  std::vector<Cand> cands;
+  for (size_t i = 0; i < std::min<size_t>(xr.size(), 12); ++i) {
+    for (size_t j = 0; j < std::min<size_t>(yr.size(), 24); ++j) {
+      std::vector<RowMap> maps;
+      if (!maps_for(xs[xr[i].second], ys[yr[j].second], &maps)) continue;
+      double c = xr[i].first + yr[j].first;
+      bool lin = true;
+      if (nst > 1) c += eval_epilogue(x, maps, nst - 2, false, nullptr, nullptr, &lin);
+      if (!lin) continue;
+      cands.push_back({c, maps});
+    }
+  }
+  if (cands.empty()) { *err = "no linear row map"; return false; }
+  std::stable_sort(cands.begin(), cands.end(),
+                   [](const Cand& a, const Cand& b) { return a.cost < b.cost; });
+
+  // Prologue item order for the best few row-map candidates: 5 lane bits
+  // among the item-coordinate bits (first three = one 8-lane phase).
+  const int lnvr = ilog2(L / R);
+  int nb;
+  if (R == 1) nb = (in_kind == ROW) ? x.g + (x.b - 2) + 2 : x.b + (x.g - 2) + 2;
+  else nb = (in_kind == ROW) ? x.g + (lnvr - 2) : lnvr + (x.g - 2);
+  const int nl = std::min(5, nb);
+  // Lane-bit pool: the low three and the top four bits of every item field
+  // (low bits pick bank groups in staging, top bits pick K positions).
+  std::vector<int> lane_pool;
+  {
+    std::vector<int> widths;
+    if (R == 1) widths = (in_kind == ROW) ? std::vector<int>{x.g, x.b - 2, 2}
+                                          : std::vector<int>{x.b, x.g - 2, 2};
+    else widths = (in_kind == ROW) ? std::vector<int>{x.g, lnvr - 2} : std::vector<int>{lnvr, x.g - 2};
+    int off = 0;
+    for (int w : widths) {
+      for (int i = 0; i < w; ++i)
+        if (i < 3 || i >= w - 4) lane_pool.push_back(off + i);
+      off += w;
+    }
+  }
+  double total_best = 1e30;
+  std::vector<int> porder_best;
+  std::vector<RowMap> maps_best;
+  const int epi_weight = 16 * nst;  // epilogue instructions per row-warp vs prologue per item-warp
+  for (size_t ci = 0; ci < std::min<size_t>(cands.size(), 4); ++ci) {
+    if (ci > 0 && cands[ci].cost > cands[0].cost + 1e-9) break;
+    double pbest = 1e30;
+    std::vector<int> porder;
+    std::vector<int> comb(nl);
+    std::function<void(int, int)> rec = [&](int start, int depth) {
+      if (pbest < 1e-9) return;
+      if (depth == nl) {
+        // which 3 of the 5 lane bits form the 8-lane phase
+        for (int m = 0; m < (1 << nl) && pbest > 1e-9; ++m) {
+          if (__builtin_popcount(m) != std::min(3, nl)) continue;
+          std::vector<int> order;
+          for (int i = 0; i < nl; ++i) if (m >> i & 1) order.push_back(comb[i]);
+          for (int i = 0; i < nl; ++i) if (!(m >> i & 1)) order.push_back(comb[i]);
+          std::set<int> u(order.begin(), order.end());
+          for (int i = 0; i < nb; ++i)
+            if (!u.count(i)) order.push_back(i);
+          bool lin = true;
+          double c = eval_prologue(x, cands[ci].maps[0], order, false, &lin);
+          if (lin && c < pbest - 1e-9) {
+            pbest = c;
+            porder = order;
+          }
+        }
+        return;
+      }
+      for (size_t i = start; i < lane_pool.size(); ++i) {
+        comb[depth] = lane_pool[i];
+        rec((int)i + 1, depth + 1);
+      }
+    };
+    rec(0, 0);
+    if (porder.empty()) continue;
+    const double total = pbest + cands[ci].cost * epi_weight / 16.0;
+    if (total < total_best - 1e-9) {
+      total_best = total;
+      porder_best = porder;
+      maps_best = cands[ci].maps;
+    }
+  }
+  if (porder_best.empty()) { *err = "no linear prologue"; return false; }
+  std::vector<RowMap> best_maps = maps_best;
+  {
+    bool lin = true;
+    p.prologue_excess = eval_prologue(x, best_maps[0], porder_best, true, &lin);
+    if (!lin) { *err = "prologue offsets are not XOR-linear"; return false; }
+  }
+  p.epi_tab.assign((size_t)nst * p.NROWS, 0);
+  p.kofs.assign((size_t)nst * 16, 0);
+  double e = 0;
+  for (int s = 0; s < nst; ++s) {
+    bool lin = true;
+    e += eval_epilogue(x, best_maps, s, true, &p.epi_tab, &p.kofs, &lin);
+    if (!lin) { *err = "epilogue offsets are not XOR-linear"; return false; }
+  }
+  p.epilogue_excess = e;
+  p.row_v.assign(nst, std::vector<uint32_t>(p.NROWS));
+  p.row_c.assign(nst, std::vector<uint32_t>(p.NROWS));
+  p.row_of.assign(nst, std::vector<uint32_t>(p.NROWS));
+  for (int s = 0; s < nst; ++s)
+    for (int v = 0; v < p.NV; ++v)
+      for (int c = 0; c < C; ++c) {
+        uint32_t r = best_maps[s].apply(v, c);
+        p.row_v[s][r] = v;
+        p.row_c[s][r] = c;
+        p.row_of[s][v * C + c] = r;
+      }
+  return true;
+}
+
+}  // namespace layout
+}  // namespace mcfft

@@ -21,6 +21,7 @@
 // directions.
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <new>
@@ -29,6 +30,7 @@
 
 #include "../../include/mcfft.h"
 #include "mcfft_internal.h"
+#include "tile_pass.h"
 
 namespace mcfft {
 namespace {
@@ -38,6 +40,8 @@ constexpr int kVersion = 100;  // 0.1.0
 enum Buf { kUserIn = 0, kUserOut = 1, kScratch = 2 };
 
 struct Pass {
+  bool tiled = false;  // TMA-fed kernel (tile_pass) instead of the direct one
+  TilePass tp;
   const PassKernel* k = nullptr;
   PassArgs a{};
   int in_buf = kUserIn, out_buf = kUserOut;
@@ -64,6 +68,8 @@ struct mcfftPlan_st {
   size_t scratch_bytes = 0;
   const uint4* bmat[2] = {nullptr, nullptr};
   const uint4* bmat_lo[2] = {nullptr, nullptr};
+  const uint4* bsw64[2] = {nullptr, nullptr};     // same matrices, 64B-swizzled layout
+  const uint4* bsw64_lo[2] = {nullptr, nullptr};
   int* status = nullptr;
   cudaStream_t last_stream = nullptr;
   mcfftPlanInfo info{};
@@ -125,7 +131,142 @@ struct PassSpec {
   int64_t in_off, out_off;
 };
 
+// Tables shared by both kernel families: stage twiddles [R'][k] (1/16 per
+// stage) and radix-R twiddles [v][k] (1/R), for both directions.
+mcfftResult make_stage_tables(mcfftPlan p, int L, int R, const float2* tw[2],
+                              const float2* tail[2]) {
+  int nst = 0;
+  for (int64_t t = L / R; t > 1; t >>= 4) ++nst;
+  int64_t tw_count = 0;
+  {
+    int64_t Ls = L / R;
+    for (int st = 0; st < nst - 1; ++st) { tw_count += Ls; Ls >>= 4; }
+  }
+  for (int dir = 0; dir < 2; ++dir) {
+    const int sign = dir == 0 ? -1 : 1;
+    if (tw_count > 0) {
+      float2* t;
+      mcfftResult r = plan_alloc(p, &t, sizeof(float2) * tw_count);
+      if (r) return r;
+      int64_t off = 0, Ls = L / R;
+      for (int st = 0; st < nst - 1; ++st) {
+        cudaError_t e = gen_twiddle_table(t + off, Ls, 0, 16, 0, Ls, sign, 1.0 / 16.0, 0);
+        if (e != cudaSuccess) return cuda_fail(e);
+        off += Ls;
+        Ls >>= 4;
+      }
+      tw[dir] = t;
+    }
+    if (R > 1) {
+      float2* t;
+      mcfftResult r = plan_alloc(p, &t, sizeof(float2) * L);
+      if (r) return r;
+      cudaError_t e = gen_twiddle_table(t, L, 0, R, 0, L, sign, 1.0 / R, 0);
+      if (e != cudaSuccess) return cuda_fail(e);
+      tail[dir] = t;
+    }
+  }
+  return MCFFT_SUCCESS;
+}
+
+// Builds a pass on the TMA-fed kernel.  Returns MCFFT_UNSUPPORTED_SIZE when
+// the shape is outside what that kernel handles (the caller falls back).
+mcfftResult add_tile_pass(mcfftPlan p, const PassSpec& s) {
+  if (p->split || std::getenv("MCFFT_NO_TILE")) return MCFFT_UNSUPPORTED_SIZE;
+  layout::Kind ik, ok;
+  if (s.in_sp == 1) ik = layout::ROW;
+  else if (s.in_sc == 1) ik = layout::COL;
+  else return MCFFT_UNSUPPORTED_SIZE;
+  if (s.out_sp == 1) ok = layout::ROW;
+  else if (s.out_sc == 1) ok = layout::COL;
+  else return MCFFT_UNSUPPORTED_SIZE;
+  // Tile size: 16K points (one CTA per SM) first unless MCFFT_TILE_POINTS
+  // says otherwise; the other size if that variant or its layout is missing.
+  int first = 16384;
+  if (const char* e = std::getenv("MCFFT_TILE_POINTS")) first = std::atoi(e);
+  const int order[2] = {first, first == 16384 ? 8192 : 16384};
+  Pass ps;
+  ps.tiled = true;
+  TilePass& tp = ps.tp;
+  const TileKernel* k = nullptr;
+  for (int oi = 0; oi < 2 && !k; ++oi) {
+    const TileKernel* cand = find_tile_kernel((int)s.L, s.posttw, p->split, order[oi]);
+    if (!cand) continue;
+    std::string err;
+    if (!tile_layout(&tp.lay, cand->L, cand->R, cand->C, ik, ok, 4, 4, s.in_sp, s.in_sc, s.in_so,
+                     s.out_sp, s.out_sc, s.out_so, s.ncols, s.nouter, &err))
+      continue;
+    if (!tile_check_encode(tp.lay.in, p->status) || !tile_check_encode(tp.lay.out, p->status))
+      continue;
+    k = cand;
+  }
+  if (!k) return MCFFT_UNSUPPORTED_SIZE;
+  tp.k = k;
+  fill_tile_args(&tp);
+  TileArgs& a = tp.args;
+  a.col_blocks = (s.ncols + k->C - 1) / k->C;
+  a.ntiles = a.col_blocks * s.nouter;
+  a.out_scale = 1.0f / 16.0f;
+  a.status = p->status;
+  // tables
+  uint2* items;
+  uint32_t* epi;
+  mcfftResult r = plan_alloc(p, &items, tp.lay.item_tab.size() * sizeof(uint32_t));
+  if (!r) r = plan_alloc(p, &epi, tp.lay.epi_tab.size() * sizeof(uint32_t));
+  if (r) return r;
+  cudaError_t e = cudaMemcpy(items, tp.lay.item_tab.data(), tp.lay.item_tab.size() * 4,
+                             cudaMemcpyHostToDevice);
+  if (e == cudaSuccess)
+    e = cudaMemcpy(epi, tp.lay.epi_tab.data(), tp.lay.epi_tab.size() * 4, cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) return cuda_fail(e);
+  a.item_tab = items;
+  a.epi_tab = epi;
+  r = make_stage_tables(p, k->L, k->R, tp.tw, tp.tail);
+  if (r) return r;
+  if (s.posttw) {
+    // two-level table for W_N^e: lo[e & (2^sh - 1)] * hi[e >> sh]
+    const int lg = ilog2(s.postN), sh = (lg + 1) / 2;
+    const int64_t nlo = int64_t(1) << sh, nhi = s.postN >> sh;
+    for (int dir = 0; dir < 2; ++dir) {
+      const int sign = dir == 0 ? -1 : 1;
+      float2 *lo, *hi;
+      r = plan_alloc(p, &lo, sizeof(float2) * nlo);
+      if (!r) r = plan_alloc(p, &hi, sizeof(float2) * nhi);
+      if (r) return r;
+      cudaError_t e2 = gen_twiddle_table(lo, nlo, 1, 0, 0, s.postN, sign, 1.0, 0);
+      if (e2 == cudaSuccess) e2 = gen_twiddle_table(hi, nhi, 1, 0, sh, s.postN, sign, 1.0, 0);
+      if (e2 != cudaSuccess) return cuda_fail(e2);
+      tp.post_a[dir] = lo;
+      tp.post_b[dir] = hi;
+    }
+    a.post_mask = (uint64_t)s.postN - 1;
+    a.post_shift = (uint32_t)sh;
+  }
+  for (int dir = 0; dir < 2; ++dir) {
+    tp.bmat[dir] = p->bsw64[dir];
+    tp.bmat_lo[dir] = p->bsw64_lo[dir];
+  }
+  int occ = 1;
+  cudaFuncSetAttribute(k->fn, cudaFuncAttributeMaxDynamicSharedMemorySize, k->smem_bytes);
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k->fn, k->nthreads, k->smem_bytes) !=
+      cudaSuccess) {
+    cudaGetLastError();
+    occ = 1;
+  }
+  occ = std::max(1, std::min(occ, 512 / k->tmem_cols));
+  tp.grid = (int)std::min<int64_t>(a.ntiles, (int64_t)p->sms * occ);
+  ps.in_buf = s.in_buf; ps.out_buf = s.out_buf;
+  ps.in_f16 = s.in_f16; ps.out_f16 = s.out_f16;
+  ps.in_off = s.in_off; ps.out_off = s.out_off;
+  p->passes.push_back(ps);
+  return MCFFT_SUCCESS;
+}
+
 mcfftResult add_pass(mcfftPlan p, const PassSpec& s) {
+  {
+    mcfftResult tr = add_tile_pass(p, s);
+    if (tr != MCFFT_UNSUPPORTED_SIZE) return tr;
+  }
   const PassKernel* k =
       pick_pass_kernel((int)s.L, s.colfast, s.posttw, p->split, s.ncols, tile_points_env());
   if (!k) return MCFFT_UNSUPPORTED_SIZE;
@@ -298,6 +439,12 @@ mcfftResult plan_begin(mcfftPlan* out, mcfftPrecision prec, unsigned flags, mcff
     if (!r) r = cuda_fail(gen_dft16_embedding(hi, lo, dir == 0 ? -1 : 1, 0));
     p->bmat[dir] = hi;
     p->bmat_lo[dir] = lo;
+    uint4 *hs = nullptr, *ls = nullptr;
+    if (!r) r = plan_alloc(p, &hs, 2048);
+    if (!r && p->split) r = plan_alloc(p, &ls, 2048);
+    if (!r) r = cuda_fail(gen_dft16_sw64(hs, ls, dir == 0 ? -1 : 1, 0));
+    p->bsw64[dir] = hs;
+    p->bsw64_lo[dir] = ls;
   }
   if (r) {
     mcfftPlanDestroy(p);
@@ -400,6 +547,20 @@ mcfftResult mcfftExec(mcfftPlan p, const void* in, void* out, int direction, voi
     const int ob = p->split ? (ps.out_f16 ? 4 : 8) : 4;
     a.in = base(ps.in_buf) + ps.in_off * ib;
     a.out = base(ps.out_buf) + ps.out_off * ob;
+    if (ps.tiled) {
+      cudaError_t e = launch_tile_pass(ps.tp, a.in, a.out, dir, st);
+      if (e == cudaSuccess && std::getenv("MCFFT_DEBUG_SYNC")) {
+        e = cudaStreamSynchronize(st);
+        fprintf(stderr, "[mcfft] tile pass L=%d R=%d C=%d grid=%d tiles=%lld: %s\n", ps.tp.k->L,
+                ps.tp.k->R, ps.tp.k->C, ps.tp.grid, (long long)ps.tp.args.ntiles,
+                cudaGetErrorString(e));
+      }
+      if (e != cudaSuccess) {
+        cudaGetLastError();
+        return MCFFT_CUDA_ERROR;
+      }
+      continue;
+    }
     a.tw = ps.tw[dir];
     a.tail_tw = ps.tail[dir];
     a.post_lo = ps.plo[dir];

@@ -61,3 +61,30 @@ cudaError_t gen_dft16_embedding(void* hi, void* lo, int sign, cudaStream_t st) {
 }
 
 }  // namespace mcfft
+
+namespace mcfft {
+
+// Same matrix as k_gen_dft16, stored in the tcgen05 K-major 64-byte-swizzled
+// layout: row j (N index) at (j>>3)*512 + (j&7)*64, 16-byte chunk q of the
+// row at ((q ^ (j>>1)) & 3) * 16, element kk at (kk & 7) * 2 within it.
+__global__ void k_gen_dft16_sw64(__half* hi, __half* lo, int sign) {
+  int t = threadIdx.x;  // 0..1023
+  int j = t >> 5, kk = t & 31;
+  int k = j >> 1, rj = j & 1, n = kk >> 1, ri = kk & 1;
+  double s, c;
+  sincospi(2.0 * (double)((k * n) % 16) / 16.0, &s, &c);
+  s *= sign;
+  double val = ri == 0 ? (rj == 0 ? c : s) : (rj == 0 ? -s : c);
+  const int q = kk >> 3;
+  const int byte = (j >> 3) * 512 + (j & 7) * 64 + (((q ^ (j >> 1)) & 3) << 4) + (kk & 7) * 2;
+  __half h = __double2half(val);
+  hi[byte / 2] = h;
+  if (lo) lo[byte / 2] = __double2half(val - (double)__half2float(h));
+}
+
+cudaError_t gen_dft16_sw64(void* hi, void* lo, int sign, cudaStream_t st) {
+  k_gen_dft16_sw64<<<1, 1024, 0, st>>>(static_cast<__half*>(hi), static_cast<__half*>(lo), sign);
+  return cudaGetLastError();
+}
+
+}  // namespace mcfft

@@ -1,0 +1,31 @@
+# Builds the reference's accuracy drivers UNCHANGED, from their sources where
+# they lie under the reference tree, against this project's compat libraries
+# (mcfft_b200/libmcfft_{1,2,3}d.so) and the FFTW-named oracle shim.  Test
+# infrastructure: outputs go to oracle/_ref/ (git-ignored; travels to the GPU
+# box).  Only builds where the reference is mounted.
+#   make -C oracle -f drivers.mk
+REF ?= /root/reference
+OUT := _ref
+CXX_ := /usr/bin/g++
+CC_ := /usr/bin/gcc
+MC := ../mcfft_b200
+FLAGS := -O2 -w -fopenmp
+
+all: $(OUT)/accuracy_1d $(OUT)/accuracy_2d $(OUT)/accuracy_3d
+
+$(OUT)/shim.o: fftw_compat/fftw_shim.c fftw_compat/fftw3.h
+	mkdir -p $(OUT)
+	$(CC_) $(FLAGS) -Ifftw_compat -c $< -o $@
+
+$(OUT)/fft64.o: fft64.c
+	mkdir -p $(OUT)
+	$(CC_) $(FLAGS) -fPIC -c $< -o $@
+
+$(OUT)/accuracy_%d: $(REF)/benchmark/accuracy_%d.cpp $(OUT)/shim.o $(OUT)/fft64.o $(MC)/libmcfft_%d.so
+	$(CXX_) $(FLAGS) -std=c++14 -Ihip_stub -Ifftw_compat $< $(OUT)/shim.o $(OUT)/fft64.o \
+	  -L$(MC) -lmcfft_$*d -Wl,-rpath,'$$ORIGIN/../../mcfft_b200' -o $@
+
+clean:
+	rm -rf $(OUT)
+
+.PHONY: all clean

