@@ -120,6 +120,23 @@ MCFFT_API mcfftResult mcfftPlanGetInfo(mcfftPlan plan, mcfftPlanInfo* info);
 MCFFT_API mcfftResult mcfftPlanDestroy(mcfftPlan plan);
 MCFFT_API const char* mcfftGetErrorString(mcfftResult result);
 
+/* Two-pass (four-step) 1D transform that allocates nothing.  No counterpart
+ * in the reference.  For callers that must not call cudaMalloc where the
+ * transform runs (a framework's caching allocator owns device memory, hosts
+ * that forbid allocation after start-up, code that cannot afford the
+ * synchronisation an allocation may imply): no plan is created and the
+ * intermediate between the two passes, the twiddle tables and the DFT-16
+ * matrix live in fixed __device__ arrays the library holds on every GPU
+ * until exit.  Plain FP16 form (as mcfftExec with MCFFT_PREC_FP16: out =
+ * DFT(in) / n), natural order, `in` and `out` distinct device buffers of
+ * n * batch FP16 complex values.  Limits: n a power of two in
+ * [2^14, 2^22], n * batch <= 2^22 (16 MiB scratch); larger sizes return
+ * MCFFT_UNSUPPORTED_SIZE or MCFFT_INVALID_VALUE.  The first call on a device
+ * looks up the arrays' device addresses and should come before any stream
+ * capture.  All calls share the arrays: calls that overlap on the GPU race. */
+MCFFT_API mcfftResult mcfftExec1dNoAlloc(const void* in, void* out, int64_t n, int64_t batch,
+                                         int direction, void* stream);
+
 /* Library version as 10000*major + 100*minor + patch. */
 MCFFT_API int mcfftGetVersion(void);
 

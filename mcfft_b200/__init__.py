@@ -39,7 +39,7 @@ FLAG_INPUT_F16 = 1
 EXPORTS = (
     "mcfftPlanCreate1d", "mcfftPlanCreate2d", "mcfftPlanCreate3d", "mcfftPlanCreateBatch",
     "mcfftExec", "mcfftPlanCheckStatus", "mcfftPlanGetInfo", "mcfftPlanDestroy",
-    "mcfftGetErrorString", "mcfftGetVersion",
+    "mcfftGetErrorString", "mcfftGetVersion", "mcfftExec1dNoAlloc",
 )
 
 
@@ -86,6 +86,8 @@ def lib() -> ctypes.CDLL:
         L.mcfftGetErrorString.argtypes = [ci]
         L.mcfftGetErrorString.restype = ctypes.c_char_p
         L.mcfftGetVersion.restype = ci
+        L.mcfftExec1dNoAlloc.argtypes = [P, P, i64, i64, ci, P]
+        L.mcfftExec1dNoAlloc.restype = ci
         for name in ("mcfftPlanCreate1d", "mcfftPlanCreate2d", "mcfftPlanCreate3d",
                      "mcfftPlanCreateBatch", "mcfftExec", "mcfftPlanCheckStatus",
                      "mcfftPlanGetInfo", "mcfftPlanDestroy"):
@@ -175,6 +177,14 @@ class Plan:
 
     def __exit__(self, *exc):
         self.close()
+
+
+def exec_1d_no_alloc(in_ptr: int, out_ptr: int, n: int, batch: int,
+                     direction: int = FORWARD, stream: int = 0):
+    """Two-pass 1D FP16 transform without any device allocation (fixed
+    device arrays inside the library; see include/mcfft.h)."""
+    _check(lib().mcfftExec1dNoAlloc(ctypes.c_void_p(in_ptr), ctypes.c_void_p(out_ptr), n, batch,
+                                    direction, ctypes.c_void_p(stream)), "mcfftExec1dNoAlloc")
 
 
 def version() -> int:

@@ -21,7 +21,8 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O2",
          "-Xcompiler", "-fvisibility=hidden", "--expt-relaxed-constexpr"]
-SOURCES = ["tables.cu", "pass_kernels.cu", "tile_pass.cu", "layout.cpp", "mcfft_api.cu"]
+SOURCES = ["tables.cu", "pass_kernels.cu", "tile_pass.cu", "layout.cpp", "mcfft_api.cu",
+           "noalloc.cu"]
 HEADERS = ["sm100_ptx.cuh", "fft_pass.cuh", "fft_pass_split.cuh", "fft_tile.cuh", "tile_pass.h",
            "layout.h", "mcfft_internal.h"]
 
