@@ -203,7 +203,7 @@ struct TileF16 {
   static constexpr int OFF_TAIL = OFF_B + 2048;
   static constexpr int OFF_TWS = OFF_TAIL + TAIL_BYTES;
   static constexpr int OFF_BAR = OFF_TWS + TWS_BYTES;
-  static constexpr int SMEM_BYTES = OFF_BAR + 128 + 1024;  // + alignment slack
+  static constexpr int SMEM_BYTES = OFF_BAR + 256 + 1024;  // + alignment slack
   static_assert(SMEM_BYTES <= 232448, "shared memory budget");
 };
 
@@ -223,16 +223,88 @@ __device__ __forceinline__ float2 twiddle2(const float2* lo, const float2* hi, u
   return cmulf(__ldg(lo + (e & ((1ull << sh) - 1))), __ldg(hi + (e >> sh)));
 }
 
+// Shared-memory address of (buffer base | buffer-relative offset) where the
+// offset is XOR-linear: (off ^ k) + base.  One LOP3 when the base is 64 KB
+// aligned (then OR equals ADD), otherwise XOR then ADD.
+__device__ __forceinline__ uint32_t xaddr(uint32_t off, uint32_t k, uint32_t base, bool or_ok) {
+  if (or_ok) {
+    uint32_t r;
+    asm("lop3.b32 %0, %1, %2, %3, 0xBE;" : "=r"(r) : "r"(off), "r"(k), "r"(base));  // (a ^ b) | c
+    return r;
+  }
+  return (off ^ k) + base;
+}
+
+// Packed-FP16 complex helpers for the plain form's radix-R stage: a __half2
+// holds (re, im).
+__device__ __forceinline__ __half2 h2swap(__half2 z) { return __lowhigh2highlow(z); }
+// z * (s i), s = +-1: (-s im, s re)
+__device__ __forceinline__ __half2 h2muli(__half2 z, __half2 negpos) {
+  return __hmul2(h2swap(z), negpos);
+}
+// z * w with w given as (wr, wr) and (-wi, wi)
+__device__ __forceinline__ __half2 h2cmul(__half2 z, __half2 wrr, __half2 wni) {
+  return __hfma2(h2swap(z), wni, __hmul2(z, wrr));
+}
+
+template <int R>
+__device__ __forceinline__ void small_dft_h2(__half2 (&x)[R], float sgn) {
+  // (-s, s) for multiplying by s*i
+  const __half2 np = __floats2half2_rn(-sgn, sgn);
+  if constexpr (R == 2) {
+    const __half2 a = x[0], b = x[1];
+    x[0] = __hadd2(a, b);
+    x[1] = __hsub2(a, b);
+  } else if constexpr (R == 4) {
+    const __half2 a0 = __hadd2(x[0], x[2]), a1 = __hsub2(x[0], x[2]);
+    const __half2 b0 = __hadd2(x[1], x[3]), b1 = h2muli(__hsub2(x[1], x[3]), np);
+    x[0] = __hadd2(a0, b0);
+    x[2] = __hsub2(a0, b0);
+    x[1] = __hadd2(a1, b1);
+    x[3] = __hsub2(a1, b1);
+  } else {
+    static_assert(R == 8, "tail radix must be 2, 4 or 8");
+    const __half2 hh = __float2half2_rn(0.70710678118654752440f);
+    __half2 e[4], o[4];
+#pragma unroll
+    for (int n = 0; n < 4; ++n) {
+      e[n] = __hadd2(x[n], x[n + 4]);
+      o[n] = __hsub2(x[n], x[n + 4]);
+    }
+    // o[n] *= W8^n, W8 = exp(s 2 pi i / 8) = h (1 + s i)
+    o[1] = __hmul2(__hadd2(o[1], h2muli(o[1], np)), hh);
+    o[2] = h2muli(o[2], np);
+    o[3] = __hmul2(__hsub2(h2muli(o[3], np), o[3]), hh);
+    small_dft_h2<4>(e, sgn);
+    small_dft_h2<4>(o, sgn);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      x[2 * k] = e[k];
+      x[2 * k + 1] = o[k];
+    }
+  }
+}
+
 template <int L, int R, int C, bool POSTTW, int NCW>
-__global__ void __launch_bounds__(NCW * 32 + 32, NCW <= 8 ? 2 : 1) fft_tile_f16(const __grid_constant__ TileArgs a) {
+// Registers are granted per block in units of four warps: 17 warps (16
+// consumers + producer) count as 20, so 65536 / 640 -> 96 per thread; the
+// 9-warp variants count as 12 warps and run two CTAs per SM -> 80.
+__global__ void __maxnreg__(NCW <= 8 ? 80 : 96) fft_tile_f16(const __grid_constant__ TileArgs a) {
   using S = TileShape<L, R, C, NCW>;
   using T = TileF16<L, R, C, POSTTW, NCW>;
   constexpr int NCT = S::NCT;
   constexpr int NIT_P = (S::ITEMS + NCT - 1) / NCT;  // prologue items per consumer thread
   constexpr int NIT_E = S::NMT * 4 / NCW;            // 32-row blocks per warp per stage
+  constexpr int NMT = S::NMT;
   static_assert(S::NMT * 4 % NCW == 0, "row blocks per warp");
+  static_assert(NMT <= 16, "per-M-tile barriers");
+  // Operand buffers alternate between the A buffer and the tile's staging
+  // buffer so that every stage's epilogue writes a buffer its MMAs do not
+  // read, and the last stage writes the staging buffer (the TMA store
+  // source).  X[s] = A when NST - s is odd, staging otherwise; with an even
+  // stage count the prologue transposes the staging buffer in place.
+  constexpr bool INPLACE_PROLOGUE = (S::NST % 2) == 0;
   extern __shared__ uint8_t smem_raw[];
-  // 1024-byte alignment for the swizzled TMA boxes and the UMMA atoms.
   const uint32_t raw_u = sm100::smem_u32(smem_raw);
   const uint32_t base_u = (raw_u + 1023u) & ~1023u;
   uint8_t* smem = smem_raw + (base_u - raw_u);
@@ -241,11 +313,14 @@ __global__ void __launch_bounds__(NCW * 32 + 32, NCW <= 8 ? 2 : 1) fft_tile_f16(
   const uint32_t sB = base_u + T::OFF_B;
   const uint32_t sTail = base_u + T::OFF_TAIL;
   const uint32_t sTws = base_u + T::OFF_TWS;
+  // OR-addressing is exact when every operand buffer starts on a multiple
+  // of its (power-of-two) size.
+  const bool or_ok = ((sS0 | sS1 | sA) & (uint32_t)(T::STAGE_BYTES - 1)) == 0;
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + T::OFF_BAR);      // [2]
   uint64_t* outrdy = full + 2;                                          // [2]
-  uint64_t* dfull = full + 4;                                           // [1]
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(full + 5);
-  volatile int* abort_flag = reinterpret_cast<volatile int*>(full + 6);
+  uint64_t* mmab = full + 4;                                            // [NMT]
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(full + 4 + 16);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(full + 4 + 17);
 
   const int tid = threadIdx.x;
   const int warp = tid >> 5, lane = tid & 31;
@@ -257,7 +332,7 @@ __global__ void __launch_bounds__(NCW * 32 + 32, NCW <= 8 ? 2 : 1) fft_tile_f16(
       sm100::mbar_init(&full[1], 1);
       sm100::mbar_init(&outrdy[0], 1);
       sm100::mbar_init(&outrdy[1], 1);
-      sm100::mbar_init(dfull, 1);
+      for (int m = 0; m < NMT; ++m) sm100::mbar_init(&mmab[m], 1);
       *abort_flag = 0;
       sm100::fence_mbar_init();
     }
@@ -268,9 +343,16 @@ __global__ void __launch_bounds__(NCW * 32 + 32, NCW <= 8 ? 2 : 1) fft_tile_f16(
     for (int i = tid; i < 128; i += NCT)
       *reinterpret_cast<uint4*>(smem + T::OFF_B + 16 * i) = __ldg(a.bmat + i);
     if constexpr (R > 1) {
-      for (int i = tid; i < L / 2; i += NCT)
-        *reinterpret_cast<float4*>(smem + T::OFF_TAIL + 16 * i) =
-            __ldg(reinterpret_cast<const float4*>(a.tail_tw) + i);
+      // radix-R twiddles as packed-FP16 pairs {(wr, wr), (-wi, wi)}
+      for (int i = tid; i < L; i += NCT) {
+        const float2 w = __ldg(a.tail_tw + i);
+        const __half2 wrr = __float2half2_rn(w.x);
+        const __half2 wni = __floats2half2_rn(-w.y, w.y);
+        uint2 v;
+        v.x = *reinterpret_cast<const uint32_t*>(&wrr);
+        v.y = *reinterpret_cast<const uint32_t*>(&wni);
+        *reinterpret_cast<uint2*>(smem + T::OFF_TAIL + 8 * i) = v;
+      }
     }
     if constexpr (T::TW_SMEM && T::TW_ENTRIES > 0) {
       for (int i = tid; i < T::TW_ENTRIES / 2; i += NCT)
@@ -334,7 +416,7 @@ __global__ void __launch_bounds__(NCW * 32 + 32, NCW <= 8 ? 2 : 1) fft_tile_f16(
     const int ctid = tid;  // 0 .. NCT-1
     const int sp = warp & 3;
     constexpr uint32_t IDESC = sm100::idesc_f16_f32(128, 32);
-    uint32_t dphase = 0;
+    uint32_t mphase = 0;  // completions of every per-M-tile barrier so far, mod 2
     const float tsgn = a.inverse ? 1.f : -1.f;
 
     // The tables are the same for every tile: keep this thread's entries in
@@ -363,49 +445,65 @@ __global__ void __launch_bounds__(NCW * 32 + 32, NCW <= 8 ? 2 : 1) fft_tile_f16(
       if (*abort_flag) break;
 
       // ---------------------------------------------------------- prologue
-      // Offsets are XOR-linear relative to their buffer: XOR first, then add
-      // the buffer base.
+      // Offsets are XOR-linear relative to their buffer.
+      const uint32_t x0 = INPLACE_PROLOGUE ? sb : sA;  // stage-0 operand buffer
+      if constexpr (R == 1) {
+        uint4 q[NIT_P][4];
 #pragma unroll
-      for (int j = 0; j < NIT_P; ++j) {
-        if (S::ITEMS % NCT != 0 && ctid + j * NCT >= S::ITEMS) break;
-        const uint2 e = ient[j];
-        const uint32_t lb = (e.x & 0xFFFFu) << 2;
-        const uint32_t st = (e.x >> 16) << 2;
-        if constexpr (R == 1) {
-          const uint4 q0 = tile::lds128(sb + (lb ^ a.lofs[0]));
-          const uint4 q1 = tile::lds128(sb + (lb ^ a.lofs[1]));
-          const uint4 q2 = tile::lds128(sb + (lb ^ a.lofs[2]));
-          const uint4 q3 = tile::lds128(sb + (lb ^ a.lofs[3]));
-          tile::sts128(sA + (st ^ a.sofs[0]), make_uint4(q0.x, q1.x, q2.x, q3.x));
-          tile::sts128(sA + (st ^ a.sofs[1]), make_uint4(q0.y, q1.y, q2.y, q3.y));
-          tile::sts128(sA + (st ^ a.sofs[2]), make_uint4(q0.z, q1.z, q2.z, q3.z));
-          tile::sts128(sA + (st ^ a.sofs[3]), make_uint4(q0.w, q1.w, q2.w, q3.w));
-        } else {
-          uint4 q[R];
+        for (int j = 0; j < NIT_P; ++j) {
+          const uint32_t lb = (ient[j].x & 0xFFFFu) << 2;
 #pragma unroll
-          for (int n = 0; n < R; ++n) q[n] = tile::lds128(sb + (lb ^ a.lofs[n]));
+          for (int n = 0; n < 4; ++n) q[j][n] = tile::lds128(xaddr(lb, a.lofs[n], sb, or_ok));
+        }
+        if (INPLACE_PROLOGUE) tile::named_bar(1, NCT);
+#pragma unroll
+        for (int j = 0; j < NIT_P; ++j) {
+          if (S::ITEMS % NCT != 0 && ctid + j * NCT >= S::ITEMS) break;
+          const uint32_t st = (ient[j].x >> 16) << 2;
+          tile::sts128(xaddr(st, a.sofs[0], x0, or_ok), make_uint4(q[j][0].x, q[j][1].x, q[j][2].x, q[j][3].x));
+          tile::sts128(xaddr(st, a.sofs[1], x0, or_ok), make_uint4(q[j][0].y, q[j][1].y, q[j][2].y, q[j][3].y));
+          tile::sts128(xaddr(st, a.sofs[2], x0, or_ok), make_uint4(q[j][0].z, q[j][1].z, q[j][2].z, q[j][3].z));
+          tile::sts128(xaddr(st, a.sofs[3], x0, or_ok), make_uint4(q[j][0].w, q[j][1].w, q[j][2].w, q[j][3].w));
+        }
+      } else {
+        uint4 q[NIT_P][R];
+#pragma unroll
+        for (int j = 0; j < NIT_P; ++j) {
+          const uint32_t lb = (ient[j].x & 0xFFFFu) << 2;
+#pragma unroll
+          for (int n = 0; n < R; ++n) q[j][n] = tile::lds128(xaddr(lb, a.lofs[n], sb, or_ok));
+        }
+        if (INPLACE_PROLOGUE) tile::named_bar(1, NCT);
+#pragma unroll
+        for (int j = 0; j < NIT_P; ++j) {
+          if (S::ITEMS % NCT != 0 && ctid + j * NCT >= S::ITEMS) break;
+          const uint32_t st = (ient[j].x >> 16) << 2;
           // item word 1: tail twiddle row of sub-vector 0; bit 31 set for
           // column items (all four sub-vectors share the row)
-          const uint32_t trow = e.y & 0x7FFFFFFFu;
-          const bool colitem = (e.y >> 31) != 0;
+          const uint32_t trow = ient[j].y & 0x7FFFFFFFu;
+          const bool colitem = (ient[j].y >> 31) != 0;
 #pragma unroll
           for (int jj = 0; jj < 4; ++jj) {
-            float2 x[R];
+            __half2 x[R];
 #pragma unroll
             for (int n = 0; n < R; ++n) {
-              const uint32_t w = jj == 0 ? q[n].x : jj == 1 ? q[n].y : jj == 2 ? q[n].z : q[n].w;
-              x[n] = sm100::unpack_half2(w);
+              const uint32_t w = jj == 0 ? q[j][n].x : jj == 1 ? q[j][n].y : jj == 2 ? q[j][n].z : q[j][n].w;
+              x[n] = *reinterpret_cast<const __half2*>(&w);
             }
-            small_dft<R>(x, tsgn);
+            small_dft_h2<R>(x, tsgn);
             const uint32_t vr = colitem ? trow : trow + jj;
             const uint32_t twa = sTail + vr * (R * 8);
 #pragma unroll
             for (int k2 = 0; k2 < R / 2; ++k2) {
-              const float4 tw4 = lds128f(twa + 16 * k2);
-              const float2 y0 = cmulf(x[2 * k2], make_float2(tw4.x, tw4.y));
-              const float2 y1 = cmulf(x[2 * k2 + 1], make_float2(tw4.z, tw4.w));
-              tile::sts32(sA + (st ^ a.sofs[jj * R + 2 * k2]), sm100::pack_half2(y0.x, y0.y));
-              tile::sts32(sA + (st ^ a.sofs[jj * R + 2 * k2 + 1]), sm100::pack_half2(y1.x, y1.y));
+              const uint4 tw = tile::lds128(twa + 16 * k2);
+              const __half2 y0 = h2cmul(x[2 * k2], *reinterpret_cast<const __half2*>(&tw.x),
+                                        *reinterpret_cast<const __half2*>(&tw.y));
+              const __half2 y1 = h2cmul(x[2 * k2 + 1], *reinterpret_cast<const __half2*>(&tw.z),
+                                        *reinterpret_cast<const __half2*>(&tw.w));
+              tile::sts32(xaddr(st, a.sofs[jj * R + 2 * k2], x0, or_ok),
+                          *reinterpret_cast<const uint32_t*>(&y0));
+              tile::sts32(xaddr(st, a.sofs[jj * R + 2 * k2 + 1], x0, or_ok),
+                          *reinterpret_cast<const uint32_t*>(&y1));
             }
           }
         }
@@ -418,45 +516,40 @@ __global__ void __launch_bounds__(NCW * 32 + 32, NCW <= 8 ? 2 : 1) fft_tile_f16(
       // ------------------------------------------------------------ stages
 #pragma unroll
       for (int s = 0; s < S::NST; ++s) {
-        constexpr bool dummy = false;
-        (void)dummy;
-        if (ctid == 0) {
-#pragma unroll 1
-          for (int m = 0; m < S::NMT; ++m) {
+        const uint32_t xs = ((S::NST - s) & 1) ? sA : sb;       // this stage's operand
+        const uint32_t xn = ((S::NST - s) & 1) ? sb : sA;       // next stage's operand
+        // Each M-tile's two MMAs and its commit are issued by lane 0 of the
+        // sub-partition-0 warp that drains that M-tile, so four warps issue
+        // in parallel (a single issuing thread serialises ~100 cycles per
+        // tcgen05.mma).  tcgen05.commit tracks the issuing thread's MMAs.
+        if (sp == 0 && lane == 0) {
+#pragma unroll
+          for (int j = 0; j < NIT_E; ++j) {
+            const uint32_t m = (warp >> 2) + j * (NCW / 4);
 #pragma unroll
             for (int ks = 0; ks < 2; ++ks)
-              sm100::umma_f16(tmem_base + 32u * m, tile::sdesc_sw64(sA + m * 8192u + ks * 32u),
+              sm100::umma_f16(tmem_base + 32u * m, tile::sdesc_sw64(xs + m * 8192u + ks * 32u),
                               tile::sdesc_sw64(sB + ks * 32u), IDESC, ks);
+            sm100::umma_commit(&mmab[m]);
           }
-          sm100::umma_commit(dfull);
         }
         const bool last = s == S::NST - 1;
         const uint32_t stw_off = stage_tw_offset<L, R>(s);
-        // Prefetch the first block's twiddles while the MMAs run (global
-        // stage tables only; shared-memory tables are read in the loop).
         float4 wpre[8];
         if (!last && !T::TW_SMEM) {
           const float4* t4 = reinterpret_cast<const float4*>(a.tw + stw_off + (eent[s][0] >> 16) * 16);
 #pragma unroll
           for (int k2 = 0; k2 < 8; ++k2) wpre[k2] = __ldg(t4 + k2);
         }
-        if (!sm100::mbar_wait_bounded(dfull, dphase, kWaitLimit)) *abort_flag = 1;
-        dphase ^= 1u;
-        sm100::tc_fence_after();
 #pragma unroll
         for (int j = 0; j < NIT_E; ++j) {
           const uint32_t m = (warp >> 2) + j * (NCW / 4);
           const uint32_t e = eent[s][j];
           const uint32_t aux = e >> 16;
           const uint32_t dst = (e & 0xFFFFu) << 2;
-          uint32_t d[32];
-          sm100::tmem_ld32(tmem_base + ((uint32_t)(32 * sp) << 16) + 32u * m, d);
-          if (!last) {
-            float4 w[8];
-            if (T::TW_SMEM) {
-#pragma unroll
-              for (int k2 = 0; k2 < 8; ++k2) w[k2] = lds128f(sTws + (stw_off + aux * 16) * 8 + 16 * k2);
-            } else if (j == 0) {
+          float4 w[8];
+          if (!last && !T::TW_SMEM) {
+            if (j == 0) {
 #pragma unroll
               for (int k2 = 0; k2 < 8; ++k2) w[k2] = wpre[k2];
             } else {
@@ -464,14 +557,31 @@ __global__ void __launch_bounds__(NCW * 32 + 32, NCW <= 8 ? 2 : 1) fft_tile_f16(
 #pragma unroll
               for (int k2 = 0; k2 < 8; ++k2) w[k2] = __ldg(t4 + k2);
             }
+          }
+          if (!sm100::mbar_wait_bounded(&mmab[m], mphase, kWaitLimit)) *abort_flag = 1;
+          sm100::tc_fence_after();
+          uint32_t d[32];
+          sm100::tmem_ld32(tmem_base + ((uint32_t)(32 * sp) << 16) + 32u * m, d);
+          if (!last) {
             sm100::tmem_wait_ld();
+            // shared-memory twiddles are read in two halves to keep eight
+            // float4 registers live instead of sixteen
 #pragma unroll
-            for (int k = 0; k < 16; ++k) {
-              const float4 ww = w[k >> 1];
-              const float2 tw = (k & 1) ? make_float2(ww.z, ww.w) : make_float2(ww.x, ww.y);
-              const float2 y =
-                  cmulf(make_float2(__uint_as_float(d[2 * k]), __uint_as_float(d[2 * k + 1])), tw);
-              tile::sts32(sA + (dst ^ a.kofs[s][k]), sm100::pack_half2(y.x, y.y));
+            for (int h = 0; h < 2; ++h) {
+              if (T::TW_SMEM) {
+#pragma unroll
+                for (int k2 = 0; k2 < 4; ++k2)
+                  w[4 * h + k2] = lds128f(sTws + (stw_off + aux * 16) * 8 + 16 * (4 * h + k2));
+              }
+#pragma unroll
+              for (int kk = 0; kk < 8; ++kk) {
+                const int k = 8 * h + kk;
+                const float4 ww = w[k >> 1];
+                const float2 tw = (k & 1) ? make_float2(ww.z, ww.w) : make_float2(ww.x, ww.y);
+                const float2 y =
+                    cmulf(make_float2(__uint_as_float(d[2 * k]), __uint_as_float(d[2 * k + 1])), tw);
+                tile::sts32(xaddr(dst, a.kofs[s][k], xn, or_ok), sm100::pack_half2(y.x, y.y));
+              }
             }
           } else if (POSTTW) {
             // Four-step twiddle W_N^((v + NV k) g): w_0 = W_N^(v g), then
@@ -490,7 +600,7 @@ __global__ void __launch_bounds__(NCW * 32 + 32, NCW <= 8 ? 2 : 1) fft_tile_f16(
             for (int k = 0; k < 16; ++k) {
               const float2 y =
                   cmulf(make_float2(__uint_as_float(d[2 * k]), __uint_as_float(d[2 * k + 1])), wk);
-              tile::sts32(sb + (dst ^ a.kofs[s][k]), sm100::pack_half2(y.x, y.y));
+              tile::sts32(xaddr(dst, a.kofs[s][k], sb, or_ok), sm100::pack_half2(y.x, y.y));
               wk = cmulf(wk, ws);
             }
           } else {
@@ -499,10 +609,11 @@ __global__ void __launch_bounds__(NCW * 32 + 32, NCW <= 8 ? 2 : 1) fft_tile_f16(
             for (int k = 0; k < 16; ++k) {
               const float yr = __uint_as_float(d[2 * k]) * a.out_scale;
               const float yi = __uint_as_float(d[2 * k + 1]) * a.out_scale;
-              tile::sts32(sb + (dst ^ a.kofs[s][k]), sm100::pack_half2(yr, yi));
+              tile::sts32(xaddr(dst, a.kofs[s][k], sb, or_ok), sm100::pack_half2(yr, yi));
             }
           }
         }
+        mphase ^= 1u;
         sm100::fence_proxy_async_smem();
         sm100::tc_fence_before();
         tile::named_bar(1, NCT);
