@@ -50,7 +50,7 @@ struct alignas(64) TileArgs {
   uint32_t lofs[8];        // XOR offsets of an item's loads
   uint32_t sofs[32];       // XOR offsets of an item's stores
   uint32_t kofs[kMaxStages][16];
-  const float2* tw;        // stage twiddles (scaled by 1/16), stages concatenated, [R'][k]
+  const float4* tw;        // stage twiddle rows (8 chunks of 16 B per R'), stages concatenated
   const float2* tail_tw;   // radix-R twiddles (scaled by 1/R), [v][k]
   const uint4* bmat;       // DFT-16 embedding (hi), 64B-swizzled K-major, 2 KB
   const uint4* bmat_lo;    // split form: low part
@@ -58,7 +58,7 @@ struct alignas(64) TileArgs {
   const float2* post_b;    // four-step: W_N^(e << post_shift) high table
   uint64_t post_mask;      // N - 1
   uint32_t post_shift;
-  float out_scale;
+  float out_scale;         // split form: applied after the last stage (the plain form keeps its 1/16 per stage in the DFT-16 matrix)
   int inverse;
   int split_in_f16;
   int* status;
@@ -175,14 +175,61 @@ struct TileShape {
   static_assert(NST >= 1 && NST <= kMaxStages, "stage count");
 };
 
-// Plain FP16 form.  Staging holds FP16 complex (4 bytes) in and out.
-// Stage twiddle entries of all non-last stages: sum of L / P_s.
+// Stage twiddle rows: one 128-byte row per R' < L_s / 16 for every stage
+// but the last, stages concatenated.  Row R' holds W_(L_s)^(k R'), k < 16,
+// as eight 16-byte chunks p = (re_2p, re_2p+1, im_2p, im_2p+1), chunk p
+// stored at position p ^ tw_fold(R') so that the few rows the lanes of a
+// warp share fall into distinct banks.
 template <int L, int R>
-constexpr int stage_tw_entries() {
+constexpr int stage_tw_rows() {
   int n = 0, Ls = L / R, nst = ilog2c(L / R) / 4;
-  for (int s = 0; s < nst - 1; ++s) { n += Ls; Ls >>= 4; }
+  for (int s = 0; s < nst - 1; ++s) { n += Ls / 16; Ls >>= 4; }
   return n;
 }
+template <int L, int R>
+__device__ __forceinline__ uint32_t stage_tw_row0(int s) {
+  uint32_t off = 0, Ls = L / R;
+  for (int i = 0; i < s; ++i) { off += Ls / 16; Ls >>= 4; }
+  return off;
+}
+__host__ __device__ __forceinline__ uint32_t tw_fold(uint32_t r) {
+  return (r ^ (r >> 3) ^ (r >> 6) ^ (r >> 9)) & 7u;
+}
+
+// Packed FP32x2 arithmetic (sm_100 f32x2 instructions) on 64-bit register
+// pairs (lo, hi).
+__device__ __forceinline__ uint64_t f2p(float lo, float hi) {
+  uint64_t r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+  return r;
+}
+__device__ __forceinline__ void f2u(uint64_t v, float& lo, float& hi) {
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+__device__ __forceinline__ uint64_t mul2(uint64_t a, uint64_t b) {
+  uint64_t r;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+__device__ __forceinline__ uint64_t sub2(uint64_t a, uint64_t b) {
+  uint64_t r;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+__device__ __forceinline__ uint64_t fma2(uint64_t a, uint64_t b, uint64_t c) {
+  uint64_t r;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
+  return r;
+}
+// Two complex products at once: (re, im) pairs of points 2p, 2p+1 times
+// the twiddle pair (wr, wi):  yr = re wr - im wi,  yi = re wi + im wr.
+__device__ __forceinline__ void cmul2(uint64_t re, uint64_t im, uint64_t wr, uint64_t wi,
+                                      uint64_t& yr, uint64_t& yi) {
+  yr = sub2(mul2(re, wr), mul2(im, wi));
+  yi = fma2(re, wi, mul2(im, wr));
+}
+
+// Plain FP16 form.  Staging holds FP16 complex (4 bytes) in and out.
 
 template <int L, int R, int C, bool POSTTW, int NCW>
 struct TileF16 {
@@ -190,12 +237,12 @@ struct TileF16 {
   static constexpr int STAGE_BYTES = L * C * 4;
   static constexpr int A_BYTES = S::NROWS * 64;
   // Twiddle tables that are constant for the whole launch live in shared
-  // memory when they are small (radix-R table always, stage tables up to
-  // 2048 entries); larger stage tables are read through L1.
-  static constexpr int TW_ENTRIES = stage_tw_entries<L, R>();
-  static constexpr bool TW_SMEM = TW_ENTRIES <= 2048;
+  // memory: the radix-R table, and the stage rows when they take at most
+  // 16 KB (all L but 4096 with R = 1, whose rows are read through L1).
+  static constexpr int TW_ROWS = stage_tw_rows<L, R>();
+  static constexpr bool TW_SMEM = TW_ROWS <= 128;
   static constexpr int TAIL_BYTES = R > 1 ? L * 8 : 0;
-  static constexpr int TWS_BYTES = TW_SMEM ? TW_ENTRIES * 8 : 0;
+  static constexpr int TWS_BYTES = TW_SMEM ? TW_ROWS * 128 : 0;
   static constexpr int OFF_S0 = 0;
   static constexpr int OFF_S1 = STAGE_BYTES;
   static constexpr int OFF_A = 2 * STAGE_BYTES;
@@ -223,16 +270,33 @@ __device__ __forceinline__ float2 twiddle2(const float2* lo, const float2* hi, u
   return cmulf(__ldg(lo + (e & ((1ull << sh) - 1))), __ldg(hi + (e >> sh)));
 }
 
-// Shared-memory address of (buffer base | buffer-relative offset) where the
-// offset is XOR-linear: (off ^ k) + base.  One LOP3 when the base is 64 KB
-// aligned (then OR equals ADD), otherwise XOR then ADD.
-__device__ __forceinline__ uint32_t xaddr(uint32_t off, uint32_t k, uint32_t base, bool or_ok) {
-  if (or_ok) {
-    uint32_t r;
-    asm("lop3.b32 %0, %1, %2, %3, 0xBE;" : "=r"(r) : "r"(off), "r"(k), "r"(base));  // (a ^ b) | c
-    return r;
-  }
-  return (off ^ k) + base;
+// Operand-buffer addressing.  Offsets inside a buffer are XOR-linear
+// (off ^ k).  The dynamic shared window starts after the 1 KB the hardware
+// reserves for the system (kWinBase), and every buffer sits at kWinBase + a
+// multiple of its own power-of-two size, so with bb = buffer - kWinBase the
+// address is ((off ^ k) | bb) + kWinBase: one LOP3, with kWinBase folded
+// into the access's immediate offset.  The kernel checks the window base
+// at entry and fails with a status code if it differs.
+constexpr uint32_t kWinBase = 1024;
+__device__ __forceinline__ uint32_t xo(uint32_t off, uint32_t k, uint32_t bb) {
+  uint32_t r;
+  asm("lop3.b32 %0, %1, %2, %3, 0xBE;" : "=r"(r) : "r"(off), "r"(k), "r"(bb));  // (a ^ b) | c
+  return r;
+}
+__device__ __forceinline__ void sts32w(uint32_t a, uint32_t v) {
+  asm volatile("st.shared.b32 [%0+1024], %1;" ::"r"(a), "r"(v) : "memory");
+}
+__device__ __forceinline__ void sts128w(uint32_t a, uint4 v) {
+  asm volatile("st.shared.v4.b32 [%0+1024], {%1,%2,%3,%4};" ::"r"(a), "r"(v.x), "r"(v.y), "r"(v.z),
+               "r"(v.w)
+               : "memory");
+}
+__device__ __forceinline__ uint4 lds128w(uint32_t a) {
+  uint4 v;
+  asm volatile("ld.shared.v4.b32 {%0,%1,%2,%3}, [%4+1024];"
+               : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
+               : "r"(a));
+  return v;
 }
 
 // Packed-FP16 complex helpers for the plain form's radix-R stage: a __half2
@@ -313,9 +377,13 @@ __global__ void __maxnreg__(NCW <= 8 ? 80 : 96) fft_tile_f16(const __grid_consta
   const uint32_t sB = base_u + T::OFF_B;
   const uint32_t sTail = base_u + T::OFF_TAIL;
   const uint32_t sTws = base_u + T::OFF_TWS;
-  // OR-addressing is exact when every operand buffer starts on a multiple
-  // of its (power-of-two) size.
-  const bool or_ok = ((sS0 | sS1 | sA) & (uint32_t)(T::STAGE_BYTES - 1)) == 0;
+  // buffer bases relative to the window base (see xo)
+  const uint32_t bS0 = sS0 - kWinBase, bS1 = sS1 - kWinBase, bA = sA - kWinBase;
+  if (((bS0 | bS1 | bA) & (uint32_t)(T::STAGE_BYTES - 1)) != 0) {
+    // a different shared-window layout than the one the addressing assumes
+    if (threadIdx.x == 0 && a.status) atomicExch(a.status, kStatusLayout);
+    return;
+  }
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + T::OFF_BAR);      // [2]
   uint64_t* outrdy = full + 2;                                          // [2]
   uint64_t* mmab = full + 4;                                            // [NMT]
@@ -354,10 +422,9 @@ __global__ void __maxnreg__(NCW <= 8 ? 80 : 96) fft_tile_f16(const __grid_consta
         *reinterpret_cast<uint2*>(smem + T::OFF_TAIL + 8 * i) = v;
       }
     }
-    if constexpr (T::TW_SMEM && T::TW_ENTRIES > 0) {
-      for (int i = tid; i < T::TW_ENTRIES / 2; i += NCT)
-        *reinterpret_cast<float4*>(smem + T::OFF_TWS + 16 * i) =
-            __ldg(reinterpret_cast<const float4*>(a.tw) + i);
+    if constexpr (T::TW_SMEM && T::TW_ROWS > 0) {
+      for (int i = tid; i < T::TW_ROWS * 8; i += NCT)
+        *reinterpret_cast<float4*>(smem + T::OFF_TWS + 16 * i) = __ldg(a.tw + i);
     }
   }
   sm100::fence_proxy_async_smem();
@@ -446,24 +513,25 @@ __global__ void __maxnreg__(NCW <= 8 ? 80 : 96) fft_tile_f16(const __grid_consta
 
       // ---------------------------------------------------------- prologue
       // Offsets are XOR-linear relative to their buffer.
-      const uint32_t x0 = INPLACE_PROLOGUE ? sb : sA;  // stage-0 operand buffer
+      const uint32_t bb = b ? bS1 : bS0;
+      const uint32_t x0 = INPLACE_PROLOGUE ? bb : bA;  // stage-0 operand buffer
       if constexpr (R == 1) {
         uint4 q[NIT_P][4];
 #pragma unroll
         for (int j = 0; j < NIT_P; ++j) {
           const uint32_t lb = (ient[j].x & 0xFFFFu) << 2;
 #pragma unroll
-          for (int n = 0; n < 4; ++n) q[j][n] = tile::lds128(xaddr(lb, a.lofs[n], sb, or_ok));
+          for (int n = 0; n < 4; ++n) q[j][n] = lds128w(xo(lb, a.lofs[n], bb));
         }
         if (INPLACE_PROLOGUE) tile::named_bar(1, NCT);
 #pragma unroll
         for (int j = 0; j < NIT_P; ++j) {
           if (S::ITEMS % NCT != 0 && ctid + j * NCT >= S::ITEMS) break;
           const uint32_t st = (ient[j].x >> 16) << 2;
-          tile::sts128(xaddr(st, a.sofs[0], x0, or_ok), make_uint4(q[j][0].x, q[j][1].x, q[j][2].x, q[j][3].x));
-          tile::sts128(xaddr(st, a.sofs[1], x0, or_ok), make_uint4(q[j][0].y, q[j][1].y, q[j][2].y, q[j][3].y));
-          tile::sts128(xaddr(st, a.sofs[2], x0, or_ok), make_uint4(q[j][0].z, q[j][1].z, q[j][2].z, q[j][3].z));
-          tile::sts128(xaddr(st, a.sofs[3], x0, or_ok), make_uint4(q[j][0].w, q[j][1].w, q[j][2].w, q[j][3].w));
+          sts128w(xo(st, a.sofs[0], x0), make_uint4(q[j][0].x, q[j][1].x, q[j][2].x, q[j][3].x));
+          sts128w(xo(st, a.sofs[1], x0), make_uint4(q[j][0].y, q[j][1].y, q[j][2].y, q[j][3].y));
+          sts128w(xo(st, a.sofs[2], x0), make_uint4(q[j][0].z, q[j][1].z, q[j][2].z, q[j][3].z));
+          sts128w(xo(st, a.sofs[3], x0), make_uint4(q[j][0].w, q[j][1].w, q[j][2].w, q[j][3].w));
         }
       } else {
         uint4 q[NIT_P][R];
@@ -471,7 +539,7 @@ __global__ void __maxnreg__(NCW <= 8 ? 80 : 96) fft_tile_f16(const __grid_consta
         for (int j = 0; j < NIT_P; ++j) {
           const uint32_t lb = (ient[j].x & 0xFFFFu) << 2;
 #pragma unroll
-          for (int n = 0; n < R; ++n) q[j][n] = tile::lds128(xaddr(lb, a.lofs[n], sb, or_ok));
+          for (int n = 0; n < R; ++n) q[j][n] = lds128w(xo(lb, a.lofs[n], bb));
         }
         if (INPLACE_PROLOGUE) tile::named_bar(1, NCT);
 #pragma unroll
@@ -500,10 +568,8 @@ __global__ void __maxnreg__(NCW <= 8 ? 80 : 96) fft_tile_f16(const __grid_consta
                                         *reinterpret_cast<const __half2*>(&tw.y));
               const __half2 y1 = h2cmul(x[2 * k2 + 1], *reinterpret_cast<const __half2*>(&tw.z),
                                         *reinterpret_cast<const __half2*>(&tw.w));
-              tile::sts32(xaddr(st, a.sofs[jj * R + 2 * k2], x0, or_ok),
-                          *reinterpret_cast<const uint32_t*>(&y0));
-              tile::sts32(xaddr(st, a.sofs[jj * R + 2 * k2 + 1], x0, or_ok),
-                          *reinterpret_cast<const uint32_t*>(&y1));
+              sts32w(xo(st, a.sofs[jj * R + 2 * k2], x0), *reinterpret_cast<const uint32_t*>(&y0));
+              sts32w(xo(st, a.sofs[jj * R + 2 * k2 + 1], x0), *reinterpret_cast<const uint32_t*>(&y1));
             }
           }
         }
@@ -517,7 +583,7 @@ __global__ void __maxnreg__(NCW <= 8 ? 80 : 96) fft_tile_f16(const __grid_consta
 #pragma unroll
       for (int s = 0; s < S::NST; ++s) {
         const uint32_t xs = ((S::NST - s) & 1) ? sA : sb;       // this stage's operand
-        const uint32_t xn = ((S::NST - s) & 1) ? sb : sA;       // next stage's operand
+        const uint32_t xn = ((S::NST - s) & 1) ? bb : bA;       // next stage's operand (window-relative)
         // Each M-tile's two MMAs and its commit are issued by lane 0 of the
         // sub-partition-0 warp that drains that M-tile, so four warps issue
         // in parallel (a single issuing thread serialises ~100 cycles per
@@ -534,82 +600,91 @@ __global__ void __maxnreg__(NCW <= 8 ? 80 : 96) fft_tile_f16(const __grid_consta
           }
         }
         const bool last = s == S::NST - 1;
-        const uint32_t stw_off = stage_tw_offset<L, R>(s);
-        float4 wpre[8];
-        if (!last && !T::TW_SMEM) {
-          const float4* t4 = reinterpret_cast<const float4*>(a.tw + stw_off + (eent[s][0] >> 16) * 16);
-#pragma unroll
-          for (int k2 = 0; k2 < 8; ++k2) wpre[k2] = __ldg(t4 + k2);
-        }
+        const uint32_t row0 = stage_tw_row0<L, R>(s);
 #pragma unroll
         for (int j = 0; j < NIT_E; ++j) {
           const uint32_t m = (warp >> 2) + j * (NCW / 4);
           const uint32_t e = eent[s][j];
           const uint32_t aux = e >> 16;
           const uint32_t dst = (e & 0xFFFFu) << 2;
-          float4 w[8];
+          // TMEM columns per lane (the DFT-16 matrix's N order): for point
+          // pair p, d[4p..4p+3] = (re_2p, re_2p+1, im_2p, im_2p+1).  The 1/16
+          // stage scale is in the matrix.
+          float4 wg[8];
           if (!last && !T::TW_SMEM) {
-            if (j == 0) {
+            const float4* t4 = a.tw + (size_t)(row0 + aux) * 8;
 #pragma unroll
-              for (int k2 = 0; k2 < 8; ++k2) w[k2] = wpre[k2];
-            } else {
-              const float4* t4 = reinterpret_cast<const float4*>(a.tw + stw_off + aux * 16);
-#pragma unroll
-              for (int k2 = 0; k2 < 8; ++k2) w[k2] = __ldg(t4 + k2);
-            }
+            for (int p = 0; p < 8; ++p) wg[p] = __ldg(t4 + (p ^ tw_fold(aux)));
           }
           if (!sm100::mbar_wait_bounded(&mmab[m], mphase, kWaitLimit)) *abort_flag = 1;
           sm100::tc_fence_after();
           uint32_t d[32];
           sm100::tmem_ld32(tmem_base + ((uint32_t)(32 * sp) << 16) + 32u * m, d);
           if (!last) {
+            const uint32_t trow = sTws + (row0 + aux) * 128u;
+            const uint32_t fold = tw_fold(aux);
             sm100::tmem_wait_ld();
-            // shared-memory twiddles are read in two halves to keep eight
-            // float4 registers live instead of sixteen
 #pragma unroll
             for (int h = 0; h < 2; ++h) {
-              if (T::TW_SMEM) {
+              float4 w[4];
 #pragma unroll
-                for (int k2 = 0; k2 < 4; ++k2)
-                  w[4 * h + k2] = lds128f(sTws + (stw_off + aux * 16) * 8 + 16 * (4 * h + k2));
-              }
+              for (int pp = 0; pp < 4; ++pp)
+                w[pp] = T::TW_SMEM ? lds128f(trow + (((4 * h + pp) ^ fold) << 4)) : wg[4 * h + pp];
 #pragma unroll
-              for (int kk = 0; kk < 8; ++kk) {
-                const int k = 8 * h + kk;
-                const float4 ww = w[k >> 1];
-                const float2 tw = (k & 1) ? make_float2(ww.z, ww.w) : make_float2(ww.x, ww.y);
-                const float2 y =
-                    cmulf(make_float2(__uint_as_float(d[2 * k]), __uint_as_float(d[2 * k + 1])), tw);
-                tile::sts32(xaddr(dst, a.kofs[s][k], xn, or_ok), sm100::pack_half2(y.x, y.y));
+              for (int pp = 0; pp < 4; ++pp) {
+                const int p = 4 * h + pp;
+                uint64_t yr, yi;
+                cmul2(f2p(__uint_as_float(d[4 * p]), __uint_as_float(d[4 * p + 1])),
+                      f2p(__uint_as_float(d[4 * p + 2]), __uint_as_float(d[4 * p + 3])),
+                      f2p(w[pp].x, w[pp].y), f2p(w[pp].z, w[pp].w), yr, yi);
+                float r0, r1, i0, i1;
+                f2u(yr, r0, r1);
+                f2u(yi, i0, i1);
+                sts32w(xo(dst, a.kofs[s][2 * p], xn), sm100::pack_half2(r0, i0));
+                sts32w(xo(dst, a.kofs[s][2 * p + 1], xn), sm100::pack_half2(r1, i1));
               }
             }
           } else if (POSTTW) {
-            // Four-step twiddle W_N^((v + NV k) g): w_0 = W_N^(v g), then
-            // w_(k+1) = w_k * W_N^(NV g) (FP32 recurrence, 15 steps, far
-            // below the FP16 output rounding).
+            // Four-step twiddle W_N^((v + NV k) g): pairs (w_2p, w_2p+1)
+            // from w_0 = W_N^(v g) and ws = W_N^(NV g), advanced by ws^2
+            // (FP32 recurrence, 7 steps, far below the FP16 output rounding).
             const uint32_t v = aux / C, c = aux % C;
             const uint64_t g = (uint64_t)(cb * C + c);
             const uint64_t e0 = ((uint64_t)v * g) & a.post_mask;
             const uint64_t es = ((uint64_t)S::NV * g) & a.post_mask;
-            float2 wk = twiddle2(a.post_a, a.post_b, e0, a.post_shift);
+            const float2 w0 = twiddle2(a.post_a, a.post_b, e0, a.post_shift);
             const float2 ws = twiddle2(a.post_a, a.post_b, es, a.post_shift);
-            wk.x *= a.out_scale;
-            wk.y *= a.out_scale;
+            const float2 w1 = cmulf(w0, ws);
+            const float2 s2 = cmulf(ws, ws);
+            uint64_t wr = f2p(w0.x, w1.x), wi = f2p(w0.y, w1.y);
+            const uint64_t s2r = f2p(s2.x, s2.x), s2i = f2p(s2.y, s2.y);
             sm100::tmem_wait_ld();
 #pragma unroll
-            for (int k = 0; k < 16; ++k) {
-              const float2 y =
-                  cmulf(make_float2(__uint_as_float(d[2 * k]), __uint_as_float(d[2 * k + 1])), wk);
-              tile::sts32(xaddr(dst, a.kofs[s][k], sb, or_ok), sm100::pack_half2(y.x, y.y));
-              wk = cmulf(wk, ws);
+            for (int p = 0; p < 8; ++p) {
+              uint64_t yr, yi;
+              cmul2(f2p(__uint_as_float(d[4 * p]), __uint_as_float(d[4 * p + 1])),
+                    f2p(__uint_as_float(d[4 * p + 2]), __uint_as_float(d[4 * p + 3])), wr, wi, yr,
+                    yi);
+              float r0, r1, i0, i1;
+              f2u(yr, r0, r1);
+              f2u(yi, i0, i1);
+              sts32w(xo(dst, a.kofs[s][2 * p], bb), sm100::pack_half2(r0, i0));
+              sts32w(xo(dst, a.kofs[s][2 * p + 1], bb), sm100::pack_half2(r1, i1));
+              if (p < 7) {
+                uint64_t nr, ni;
+                cmul2(wr, wi, s2r, s2i, nr, ni);
+                wr = nr;
+                wi = ni;
+              }
             }
           } else {
             sm100::tmem_wait_ld();
 #pragma unroll
-            for (int k = 0; k < 16; ++k) {
-              const float yr = __uint_as_float(d[2 * k]) * a.out_scale;
-              const float yi = __uint_as_float(d[2 * k + 1]) * a.out_scale;
-              tile::sts32(xaddr(dst, a.kofs[s][k], sb, or_ok), sm100::pack_half2(yr, yi));
+            for (int p = 0; p < 8; ++p) {
+              sts32w(xo(dst, a.kofs[s][2 * p], bb),
+                     sm100::pack_half2(__uint_as_float(d[4 * p]), __uint_as_float(d[4 * p + 2])));
+              sts32w(xo(dst, a.kofs[s][2 * p + 1], bb),
+                     sm100::pack_half2(__uint_as_float(d[4 * p + 1]), __uint_as_float(d[4 * p + 3])));
             }
           }
         }

@@ -132,7 +132,8 @@ struct PassSpec {
 };
 
 // Tables shared by both kernel families: stage twiddles [R'][k] (1/16 per
-// stage) and radix-R twiddles [v][k] (1/R), for both directions.
+// stage; skipped when tw is null) and radix-R twiddles [v][k] (1/R), for
+// both directions.
 mcfftResult make_stage_tables(mcfftPlan p, int L, int R, const float2* tw[2],
                               const float2* tail[2]) {
   int nst = 0;
@@ -144,7 +145,7 @@ mcfftResult make_stage_tables(mcfftPlan p, int L, int R, const float2* tw[2],
   }
   for (int dir = 0; dir < 2; ++dir) {
     const int sign = dir == 0 ? -1 : 1;
-    if (tw_count > 0) {
+    if (tw_count > 0 && tw) {
       float2* t;
       mcfftResult r = plan_alloc(p, &t, sizeof(float2) * tw_count);
       if (r) return r;
@@ -165,6 +166,33 @@ mcfftResult make_stage_tables(mcfftPlan p, int L, int R, const float2* tw[2],
       if (e != cudaSuccess) return cuda_fail(e);
       tail[dir] = t;
     }
+  }
+  return MCFFT_SUCCESS;
+}
+
+// Stage twiddle rows of the tile kernel, both directions: for every stage
+// but the last, W^(k R') with W = exp(-+2 pi i / L_s), R' < L_s/16, k < 16.
+mcfftResult make_stage_rows(mcfftPlan p, int L, int R, const float4* tw[2]) {
+  int nst = 0;
+  for (int64_t t = L / R; t > 1; t >>= 4) ++nst;
+  int64_t count = 0;
+  {
+    int64_t Ls = L / R;
+    for (int st = 0; st < nst - 1; ++st) { count += Ls / 16; Ls >>= 4; }
+  }
+  if (count == 0) return MCFFT_SUCCESS;
+  for (int dir = 0; dir < 2; ++dir) {
+    float4* t;
+    mcfftResult r = plan_alloc(p, &t, sizeof(float4) * 8 * count);
+    if (r) return r;
+    int64_t off = 0, Ls = L / R;
+    for (int st = 0; st < nst - 1; ++st) {
+      cudaError_t e = gen_stage_rows(t + 8 * off, Ls / 16, Ls, dir == 0 ? -1 : 1, 0);
+      if (e != cudaSuccess) return cuda_fail(e);
+      off += Ls / 16;
+      Ls >>= 4;
+    }
+    tw[dir] = t;
   }
   return MCFFT_SUCCESS;
 }
@@ -206,7 +234,7 @@ mcfftResult add_tile_pass(mcfftPlan p, const PassSpec& s) {
   TileArgs& a = tp.args;
   a.col_blocks = (s.ncols + k->C - 1) / k->C;
   a.ntiles = a.col_blocks * s.nouter;
-  a.out_scale = 1.0f / 16.0f;
+  a.out_scale = 1.0f;  // the last stage's 1/16 is in the DFT-16 matrix
   a.status = p->status;
   // tables
   uint2* items;
@@ -221,7 +249,9 @@ mcfftResult add_tile_pass(mcfftPlan p, const PassSpec& s) {
   if (e != cudaSuccess) return cuda_fail(e);
   a.item_tab = items;
   a.epi_tab = epi;
-  r = make_stage_tables(p, k->L, k->R, tp.tw, tp.tail);
+  r = make_stage_tables(p, k->L, k->R, nullptr, tp.tail);
+  if (r) return r;
+  r = make_stage_rows(p, k->L, k->R, tp.tw);
   if (r) return r;
   if (s.posttw) {
     // two-level table for W_N^e: lo[e & (2^sh - 1)] * hi[e >> sh]
@@ -442,7 +472,10 @@ mcfftResult plan_begin(mcfftPlan* out, mcfftPrecision prec, unsigned flags, mcff
     uint4 *hs = nullptr, *ls = nullptr;
     if (!r) r = plan_alloc(p, &hs, 2048);
     if (!r && p->split) r = plan_alloc(p, &ls, 2048);
-    if (!r) r = cuda_fail(gen_dft16_sw64(hs, ls, dir == 0 ? -1 : 1, 0));
+    // The tile kernel's plain form folds the 1/16 stage scale into the
+    // matrix (exact: a power of two); the split form keeps it unscaled so
+    // the low part stays in FP16's normal range.
+    if (!r) r = cuda_fail(gen_dft16_sw64(hs, ls, dir == 0 ? -1 : 1, p->split ? 1.0 : 1.0 / 16.0, 0));
     p->bsw64[dir] = hs;
     p->bsw64_lo[dir] = ls;
   }
@@ -586,7 +619,7 @@ mcfftResult mcfftPlanCheckStatus(mcfftPlan p) {
     return MCFFT_CUDA_ERROR;
   if (h != kStatusOk) {
     cudaMemset(p->status, 0, sizeof(int));
-    return MCFFT_DEVICE_TIMEOUT;
+    return h == kStatusTimeout ? MCFFT_DEVICE_TIMEOUT : MCFFT_INTERNAL_ERROR;
   }
   return MCFFT_SUCCESS;
 }

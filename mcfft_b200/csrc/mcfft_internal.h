@@ -10,6 +10,7 @@ namespace mcfft {
 // Device status word values (written by kernels with atomicExch).
 constexpr int kStatusOk = 0;
 constexpr int kStatusTimeout = 1;
+constexpr int kStatusLayout = 2;  // shared-memory window not where the kernel's addressing expects
 
 // Arguments of one pass kernel launch.  All strides are in complex
 // elements.  Element (tile, point p, column c) lives at

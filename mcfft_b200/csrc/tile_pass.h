@@ -25,7 +25,7 @@ struct TilePass {
   layout::PassLayout lay;
   TileArgs args{};  // everything except tensor maps and per-direction tables
   int grid = 1;
-  const float2* tw[2] = {nullptr, nullptr};
+  const float4* tw[2] = {nullptr, nullptr};
   const float2* tail[2] = {nullptr, nullptr};
   const float2* post_a[2] = {nullptr, nullptr};
   const float2* post_b[2] = {nullptr, nullptr};
@@ -42,8 +42,12 @@ void fill_tile_args(TilePass* tp);
 cudaError_t launch_tile_pass(const TilePass& tp, const void* in, void* out, int dir,
                              cudaStream_t st);
 
-// DFT-16 embedding in the 64-byte-swizzled K-major layout the tile kernel
-// reads (row j = output component, K = 16 interleaved complex inputs).
-cudaError_t gen_dft16_sw64(void* hi, void* lo, int sign, cudaStream_t st);
+// DFT-16 embedding times `scale` (a power of two) in the 64-byte-swizzled
+// K-major layout the tile kernel reads (row j = output component, K = 16
+// interleaved complex inputs).
+cudaError_t gen_dft16_sw64(void* hi, void* lo, int sign, double scale, cudaStream_t st);
+// Stage twiddle rows (W^(k R'), k < 16, chunked and swizzled for the tile
+// kernel), W = exp(sign 2 pi i / modulus), R' < rows.
+cudaError_t gen_stage_rows(float4* dst, int64_t rows, int64_t modulus, int sign, cudaStream_t st);
 
 }  // namespace mcfft
