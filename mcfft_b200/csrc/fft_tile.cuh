@@ -47,7 +47,7 @@ struct alignas(64) TileArgs {
   uint32_t in_tile_bytes;
   const uint2* item_tab;   // per prologue item: {lds_base>>2 | sts_base>>2 << 16, tail twiddle row}
   const uint32_t* epi_tab; // [stage][row]: dst_base>>2 | aux << 16
-  uint32_t lofs[8];        // XOR offsets of an item's loads
+  uint32_t lofs[16];       // XOR offsets of an item's loads
   uint32_t sofs[32];       // XOR offsets of an item's stores
   uint32_t kofs[kMaxStages][16];
   const float4* tw;        // stage twiddle rows (8 chunks of 16 B per R'), stages concatenated

@@ -259,7 +259,11 @@ double eval_prologue(const Ctx& x, const RowMap& m0, const std::vector<int>& ord
     f[1] = (cbits >> widths[0]) & ((1u << widths[1]) - 1);
     f[2] = (cbits >> (widths[0] + widths[1])) & ((1u << widths[2]) - 1);
   };
-  const int nl = p.R == 1 ? 4 : p.R;            // loads per item
+  // A 16-byte load covers 4 FP16 or 2 FP32 complex points: with FP32
+  // staging each point group of an item takes two loads (halves h = 0, 1,
+  // the second two points / columns), and load index j = group * nh + h.
+  const int nh = p.in.elem == 8 ? 2 : 1;
+  const int nl = (p.R == 1 ? 4 : p.R) * nh;     // loads per item
   const int ns = p.R == 1 ? 4 : 4 * p.R;        // stores per item
   const int sbytes = p.R == 1 ? 16 : 4;
   std::vector<uint32_t> lb(nitems), sb(nitems), tw(nitems);
@@ -271,13 +275,14 @@ double eval_prologue(const Ctx& x, const RowMap& m0, const std::vector<int>& ord
     uint32_t f[3];
     coords(it, f);
     for (int j = 0; j < nl; ++j) {
+      const uint32_t jg = j / nh, h2 = 2 * (j % nh);
       uint32_t pos, c;
       if (p.R == 1) {
-        if (p.in_kind == ROW) { c = f[0]; pos = (4 * f[2] + j) * p.NV + 4 * f[1]; }
-        else { c = 4 * f[1]; pos = (4 * f[2] + j) * p.NV + f[0]; }
+        if (p.in_kind == ROW) { c = f[0]; pos = (4 * f[2] + jg) * p.NV + 4 * f[1] + h2; }
+        else { c = 4 * f[1] + h2; pos = (4 * f[2] + jg) * p.NV + f[0]; }
       } else {
-        if (p.in_kind == ROW) { c = f[0]; pos = j * NVR + 4 * f[1]; }
-        else { c = 4 * f[1]; pos = j * NVR + f[0]; }
+        if (p.in_kind == ROW) { c = f[0]; pos = jg * NVR + 4 * f[1] + h2; }
+        else { c = 4 * f[1] + h2; pos = jg * NVR + f[0]; }
       }
       la[(size_t)it * nl + j] = p.in.offset(pos, c);
     }

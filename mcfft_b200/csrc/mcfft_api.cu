@@ -172,7 +172,7 @@ mcfftResult make_stage_tables(mcfftPlan p, int L, int R, const float2* tw[2],
 
 // Stage twiddle rows of the tile kernel, both directions: for every stage
 // but the last, W^(k R') with W = exp(-+2 pi i / L_s), R' < L_s/16, k < 16.
-mcfftResult make_stage_rows(mcfftPlan p, int L, int R, const float4* tw[2]) {
+mcfftResult make_stage_rows(mcfftPlan p, int L, int R, double scale, const float4* tw[2]) {
   int nst = 0;
   for (int64_t t = L / R; t > 1; t >>= 4) ++nst;
   int64_t count = 0;
@@ -187,7 +187,7 @@ mcfftResult make_stage_rows(mcfftPlan p, int L, int R, const float4* tw[2]) {
     if (r) return r;
     int64_t off = 0, Ls = L / R;
     for (int st = 0; st < nst - 1; ++st) {
-      cudaError_t e = gen_stage_rows(t + 8 * off, Ls / 16, Ls, dir == 0 ? -1 : 1, 0);
+      cudaError_t e = gen_stage_rows(t + 8 * off, Ls / 16, Ls, dir == 0 ? -1 : 1, scale, 0);
       if (e != cudaSuccess) return cuda_fail(e);
       off += Ls / 16;
       Ls >>= 4;
@@ -200,7 +200,7 @@ mcfftResult make_stage_rows(mcfftPlan p, int L, int R, const float4* tw[2]) {
 // Builds a pass on the TMA-fed kernel.  Returns MCFFT_UNSUPPORTED_SIZE when
 // the shape is outside what that kernel handles (the caller falls back).
 mcfftResult add_tile_pass(mcfftPlan p, const PassSpec& s) {
-  if (p->split || std::getenv("MCFFT_NO_TILE")) return MCFFT_UNSUPPORTED_SIZE;
+  if (std::getenv("MCFFT_NO_TILE")) return MCFFT_UNSUPPORTED_SIZE;
   layout::Kind ik, ok;
   if (s.in_sp == 1) ik = layout::ROW;
   else if (s.in_sc == 1) ik = layout::COL;
@@ -208,21 +208,27 @@ mcfftResult add_tile_pass(mcfftPlan p, const PassSpec& s) {
   if (s.out_sp == 1) ok = layout::ROW;
   else if (s.out_sc == 1) ok = layout::COL;
   else return MCFFT_UNSUPPORTED_SIZE;
-  // Tile size: 16K points (one CTA per SM) first unless MCFFT_TILE_POINTS
-  // says otherwise; the other size if that variant or its layout is missing.
+  // Tile size: plain form 16K points (one CTA per SM) first unless
+  // MCFFT_TILE_POINTS says otherwise, the other size if that variant or its
+  // layout is missing; split form 8K points (its FP32 staging is twice as
+  // large per point).
   int first = 16384;
   if (const char* e = std::getenv("MCFFT_TILE_POINTS")) first = std::atoi(e);
-  const int order[2] = {first, first == 16384 ? 8192 : 16384};
+  const int order[2] = {p->split ? 8192 : first,
+                        p->split ? 8192 : (first == 16384 ? 8192 : 16384)};
+  const int in_elem = s.in_f16 ? 4 : 8, out_elem = s.out_f16 ? 4 : 8;
   Pass ps;
   ps.tiled = true;
   TilePass& tp = ps.tp;
   const TileKernel* k = nullptr;
   for (int oi = 0; oi < 2 && !k; ++oi) {
-    const TileKernel* cand = find_tile_kernel((int)s.L, s.posttw, p->split, order[oi]);
+    const TileKernel* cand =
+        find_tile_kernel((int)s.L, s.posttw, p->split, order[oi], s.in_f16 != 0);
     if (!cand) continue;
+    if (!p->split && (in_elem != 4 || out_elem != 4)) continue;
     std::string err;
-    if (!tile_layout(&tp.lay, cand->L, cand->R, cand->C, ik, ok, 4, 4, s.in_sp, s.in_sc, s.in_so,
-                     s.out_sp, s.out_sc, s.out_so, s.ncols, s.nouter, &err))
+    if (!tile_layout(&tp.lay, cand->L, cand->R, cand->C, ik, ok, in_elem, out_elem, s.in_sp,
+                     s.in_sc, s.in_so, s.out_sp, s.out_sc, s.out_so, s.ncols, s.nouter, &err))
       continue;
     if (!tile_check_encode(tp.lay.in, p->status) || !tile_check_encode(tp.lay.out, p->status))
       continue;
@@ -234,7 +240,8 @@ mcfftResult add_tile_pass(mcfftPlan p, const PassSpec& s) {
   TileArgs& a = tp.args;
   a.col_blocks = (s.ncols + k->C - 1) / k->C;
   a.ntiles = a.col_blocks * s.nouter;
-  a.out_scale = 1.0f;  // the last stage's 1/16 is in the DFT-16 matrix
+  a.out_scale = 1.0f;  // unused: the plain form's last 1/16 is in the DFT-16 matrix,
+                       // the split form derives its output factor per tile
   a.status = p->status;
   // tables
   uint2* items;
@@ -251,7 +258,9 @@ mcfftResult add_tile_pass(mcfftPlan p, const PassSpec& s) {
   a.epi_tab = epi;
   r = make_stage_tables(p, k->L, k->R, nullptr, tp.tail);
   if (r) return r;
-  r = make_stage_rows(p, k->L, k->R, tp.tw);
+  // stage rows: the plain form's 1/16 is in its DFT-16 matrix, the split
+  // form's in the rows
+  r = make_stage_rows(p, k->L, k->R, p->split ? 1.0 / 16.0 : 1.0, tp.tw);
   if (r) return r;
   if (s.posttw) {
     // two-level table for W_N^e: lo[e & (2^sh - 1)] * hi[e >> sh]

@@ -93,11 +93,12 @@ cudaError_t gen_dft16_sw64(void* hi, void* lo, int sign, double scale, cudaStrea
 }
 
 // Stage twiddle rows of the tile kernel: for R' < rows, row R' holds
-// W^(k R'), W = exp(sign 2 pi i / modulus), k < 16, as eight chunks
+// scale * W^(k R'), W = exp(sign 2 pi i / modulus), k < 16, as eight chunks
 // p = (re_2p, re_2p+1, im_2p, im_2p+1); chunk p is stored at position
 // p ^ fold(R'), fold(r) = (r ^ r>>3 ^ r>>6 ^ r>>9) & 7 (the kernel's
 // tw_fold).
-__global__ void k_gen_stage_rows(float4* dst, int64_t rows, int64_t modulus, int sign) {
+__global__ void k_gen_stage_rows(float4* dst, int64_t rows, int64_t modulus, int sign,
+                                 double scale) {
   const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (t >= rows * 8) return;
   const int64_t r = t >> 3;
@@ -109,15 +110,16 @@ __global__ void k_gen_stage_rows(float4* dst, int64_t rows, int64_t modulus, int
   }
   const uint32_t ru = (uint32_t)r;
   const uint32_t fold = (ru ^ (ru >> 3) ^ (ru >> 6) ^ (ru >> 9)) & 7u;
-  dst[r * 8 + (p ^ fold)] =
-      make_float4((float)c[0], (float)c[1], (float)(sign * s[0]), (float)(sign * s[1]));
+  dst[r * 8 + (p ^ fold)] = make_float4((float)(scale * c[0]), (float)(scale * c[1]),
+                                        (float)(scale * sign * s[0]), (float)(scale * sign * s[1]));
 }
 
-cudaError_t gen_stage_rows(float4* dst, int64_t rows, int64_t modulus, int sign, cudaStream_t st) {
+cudaError_t gen_stage_rows(float4* dst, int64_t rows, int64_t modulus, int sign, double scale,
+                           cudaStream_t st) {
   if (rows <= 0) return cudaSuccess;
   const int threads = 256;
   const int64_t blocks = (rows * 8 + threads - 1) / threads;
-  k_gen_stage_rows<<<(unsigned)blocks, threads, 0, st>>>(dst, rows, modulus, sign);
+  k_gen_stage_rows<<<(unsigned)blocks, threads, 0, st>>>(dst, rows, modulus, sign, scale);
   return cudaGetLastError();
 }
 

@@ -25,7 +25,7 @@ TileKernel make_f16() {
   using T = TileF16<L, R, C, PT, NCW>;
   using S = TileShape<L, R, C, NCW>;
   return TileKernel{reinterpret_cast<const void*>(&fft_tile_f16<L, R, C, PT, NCW>),
-                    L, R, C, PT, false, S::NT, T::SMEM_BYTES, S::TMEM_COLS, TP};
+                    L, R, C, PT, false, S::NT, T::SMEM_BYTES, S::TMEM_COLS, TP, true};
 }
 
 #define MCFFT_TILE_VARIANTS(PT, TP, NCW)                                                  \
@@ -91,9 +91,9 @@ std::map<std::string, layout::PassLayout> g_lay_cache;
 
 }  // namespace
 
-const TileKernel* find_tile_kernel(int L, bool posttw, bool split, int tile_points) {
-  for (const auto& k : registry())
-    if (k.L == L && k.posttw == posttw && k.split == split && k.tile_points == tile_points)
+const TileKernel* find_tile_kernel(int L, bool posttw, bool split, int tile_points, bool in16) {
+  for (const auto& k : split ? split_registry() : registry())
+    if (k.L == L && k.posttw == posttw && k.tile_points == tile_points && (!split || k.in16 == in16))
       return &k;
   return nullptr;
 }
@@ -169,7 +169,7 @@ void fill_tile_args(TilePass* tp) {
     a.out_omul[d] = l.out.omul[d];
   }
   a.in_tile_bytes = l.in.bytes();
-  for (size_t i = 0; i < l.lofs.size() && i < 8; ++i) a.lofs[i] = l.lofs[i];
+  for (size_t i = 0; i < l.lofs.size() && i < 16; ++i) a.lofs[i] = l.lofs[i];
   for (size_t i = 0; i < l.sofs.size() && i < 32; ++i) a.sofs[i] = l.sofs[i];
   for (int s = 0; s < l.NST && s < kMaxStages; ++s)
     for (int k = 0; k < 16; ++k) a.kofs[s][k] = l.kofs[(size_t)s * 16 + k];

@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <string>
+#include <vector>
 
 #include "fft_tile.cuh"
 #include "layout.h"
@@ -17,7 +18,11 @@ struct TileKernel {
   int smem_bytes;
   int tmem_cols;
   int tile_points;
+  bool in16;  // split form: FP16 input staging (FP32 otherwise); plain: always
 };
+
+// Split-form variants (tile_split.cu).
+const std::vector<TileKernel>& split_registry();
 
 // One pass of a plan executed by the TMA-fed kernel.
 struct TilePass {
@@ -33,7 +38,7 @@ struct TilePass {
   const uint4* bmat_lo[2] = {nullptr, nullptr};
 };
 
-const TileKernel* find_tile_kernel(int L, bool posttw, bool split, int tile_points);
+const TileKernel* find_tile_kernel(int L, bool posttw, bool split, int tile_points, bool in16);
 bool tile_layout(layout::PassLayout* out, int L, int R, int C, layout::Kind ik, layout::Kind ok,
                  int in_elem, int out_elem, int64_t isp, int64_t isc, int64_t iso, int64_t osp,
                  int64_t osc, int64_t oso, int64_t ncols, int64_t nouter, std::string* err);
@@ -46,8 +51,9 @@ cudaError_t launch_tile_pass(const TilePass& tp, const void* in, void* out, int 
 // K-major layout the tile kernel reads (row j = output component, K = 16
 // interleaved complex inputs).
 cudaError_t gen_dft16_sw64(void* hi, void* lo, int sign, double scale, cudaStream_t st);
-// Stage twiddle rows (W^(k R'), k < 16, chunked and swizzled for the tile
-// kernel), W = exp(sign 2 pi i / modulus), R' < rows.
-cudaError_t gen_stage_rows(float4* dst, int64_t rows, int64_t modulus, int sign, cudaStream_t st);
+// Stage twiddle rows (scale * W^(k R'), k < 16, chunked and swizzled for
+// the tile kernel), W = exp(sign 2 pi i / modulus), R' < rows.
+cudaError_t gen_stage_rows(float4* dst, int64_t rows, int64_t modulus, int sign, double scale,
+                           cudaStream_t st);
 
 }  // namespace mcfft
