@@ -133,6 +133,54 @@ def time_steps(fn, steps, warmup, torch, stream, barrier):
     return total / steps, per
 
 
+def uneven_shapes(seed=4):
+    """The uneven-batch workload: 4096 1D transforms with N = 2^e, e uniform
+    in 8..16, and 64 2D transforms with Nx, Ny uniform in {128, 256, 512}
+    (numpy PCG64, seed 4), ordered by shape so that equal shapes lie
+    contiguously (the plan batches them)."""
+    rng = np.random.default_rng(seed)
+    e = rng.integers(8, 17, 4096)
+    sides = np.array([128, 256, 512])
+    nx = sides[rng.integers(0, 3, 64)]
+    ny = sides[rng.integers(0, 3, 64)]
+    shapes = [(1 << int(k),) for k in e] + [(int(a), int(b)) for a, b in zip(nx, ny)]
+    return sorted(shapes, key=lambda s: (len(s), s))
+
+
+def bench_uneven(args, torch, mc, stream, barrier, peak):
+    """Both forms on the uneven batch: one plan over 4160 descriptors (one
+    per transform); returns its timings next to the summed ideal HBM time
+    (one read of the input plus one write of the output at `peak`)."""
+    shapes = uneven_shapes()
+    descs, off = [], 0
+    for s in shapes:
+        n = int(np.prod(s))
+        descs.append((s, 1, off, off))
+        off += n
+    total = off
+    flops = sum(5.0 * np.prod(s) * np.log2(np.prod(s)) for s in shapes)
+    rng = np.random.default_rng(4)
+    host = rng.uniform(-1, 1, 2 * total).astype(np.float16)
+    x = torch.from_numpy(host.view(np.uint16)).to("cuda").view(torch.complex32)
+    out = {"workload": "4096 1D transforms N=2^8..2^16 + 64 2D transforms with 128..512 sides "
+                       "(seed 4), forward", "transforms": len(shapes), "points": total}
+    sptr = stream.cuda_stream
+    for name, prec, flags, obytes in (("plain", mc.PREC_FP16, mc.FLAG_NONE, 4),
+                                      ("split", mc.PREC_SPLIT, mc.FLAG_INPUT_F16, 8)):
+        y = torch.empty(total * obytes // 4, dtype=torch.complex32, device="cuda")
+        with mc.Plan(descs=descs, precision=prec, flags=flags) as p:
+            info = p.info()
+            ms, _ = time_steps(lambda: p.exec_ptr(x.data_ptr(), y.data_ptr(), mc.FORWARD, sptr),
+                               args.steps, args.warmup, torch, stream, barrier)
+            p.check_status()
+        ideal_ms = total * (4 + obytes) / (peak * 1e9) * 1e3
+        out[name] = {"ms_per_exec": round(ms, 4), "gflops": round(flops / (ms * 1e-3) / 1e9, 1),
+                     "ideal_hbm_ms": round(ideal_ms, 4), "vs_ideal": round(ms / ideal_ms, 3),
+                     "launches_per_exec": info.launches, "passes": info.num_passes}
+        del y
+    return out
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
 
@@ -257,6 +305,10 @@ def run_ours(args, rank, world, local_rank):
             "gpu_launches": info.num_passes * args.steps,
             "clocks": clocks,
         }
+    if args.config == "c2" and not args.no_uneven:
+        ub = bench_uneven(args, torch, mc, stream, barrier, peak)
+        if result is not None:
+            result["uneven_batch"] = ub
     plan.close()
     splan.close()
     return result, host, dims, batch
@@ -323,6 +375,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="c2", choices=sorted(CONFIGS))
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-uneven", action="store_true", help="skip the uneven-batch leg")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 

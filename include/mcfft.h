@@ -94,6 +94,7 @@ typedef struct {
   int64_t out_bytes;       /* bytes written to the output per exec */
   int64_t workspace_bytes; /* device scratch held by the plan */
   int num_descs;           /* transform groups (mcfftPlanCreateBatch) */
+  int launches;            /* this library's kernel launches per exec (1: batch queue) */
 } mcfftPlanInfo;
 
 MCFFT_API mcfftResult mcfftPlanCreate1d(mcfftPlan* plan, int64_t n, int64_t batch,

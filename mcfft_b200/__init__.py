@@ -59,7 +59,8 @@ class PlanInfo(ctypes.Structure):
                 ("precision", ctypes.c_int), ("num_passes", ctypes.c_int),
                 ("scale_log2", ctypes.c_int), ("elements", ctypes.c_int64),
                 ("in_bytes", ctypes.c_int64), ("out_bytes", ctypes.c_int64),
-                ("workspace_bytes", ctypes.c_int64), ("num_descs", ctypes.c_int)]
+                ("workspace_bytes", ctypes.c_int64), ("num_descs", ctypes.c_int),
+                ("launches", ctypes.c_int)]
 
 
 _lib = None

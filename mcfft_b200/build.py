@@ -21,10 +21,11 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O2",
          "-Xcompiler", "-fvisibility=hidden", "--expt-relaxed-constexpr"]
-SOURCES = ["tables.cu", "pass_kernels.cu", "tile_pass.cu", "tile_split.cu", "layout.cpp",
-           "mcfft_api.cu", "noalloc.cu"]
+SOURCES = ["tables.cu", "pass_kernels.cu", "tile_pass.cu", "tile_split.cu", "queue.cu",
+           "layout.cpp", "mcfft_api.cu", "noalloc.cu"]
 HEADERS = ["sm100_ptx.cuh", "fft_pass.cuh", "fft_pass_split.cuh", "fft_tile.cuh",
-           "fft_tile_split.cuh", "tile_pass.h", "layout.h", "mcfft_internal.h"]
+           "fft_tile_split.cuh", "fft_queue.cuh", "queue.h", "tile_pass.h", "layout.h",
+           "mcfft_internal.h"]
 
 
 def _stale(target: str, deps) -> bool:

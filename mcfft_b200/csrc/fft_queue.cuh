@@ -1,0 +1,343 @@
+// fft_queue.cuh -- persistent batch kernel: one launch runs every pass of a
+// plan (many transforms of uneven lengths and dimensionality) from a device
+// work queue of (pass, tile) items, plain FP16 form.
+//
+// Each CTA takes items blockIdx.x, blockIdx.x + gridDim.x, ... of the queue
+// in order.  Per item the producer warp issues the TMA load of the tile's
+// input and, once the consumers are done, the TMA store of its output; the
+// consumer warps run the same per-tile routine as the per-pass kernel
+// (F16Tile::run), instantiated for every pass variant (L, four-step
+// twiddle) and selected per item.  Layout tables and tensor maps of all
+// passes live in the kernel's parameter block (constant bank).
+//
+// Dependencies between passes of one transform (the second pass of a
+// four-step 1D transform, the column passes of 2D/3D transforms) go through
+// counters in global memory: after its output tile is written, a producing
+// tile adds 1 to the counter of every key (transform / slab) it covers; the
+// producer warp of a consuming tile polls its key's counter until it holds
+// the producing pass's tile count before loading.  The host orders the
+// queue so that every dependency points to an earlier item, the kernel is
+// launched cooperatively (all CTAs resident), and the producer never blocks
+// its own stores while it waits for a dependency, so every wait ends.  All
+// waits are bounded; on timeout the kernel records kStatusTimeout.
+//
+// Memory ordering of a dependency: writer = bulk store, wait for its
+// completion (cp.async.bulk.wait_group 0), proxy fence, release add;
+// reader = acquire load, proxy fence, bulk tensor load.
+#pragma once
+#include "fft_tile.cuh"
+
+namespace mcfft {
+
+constexpr int kQueueMaxPasses = 33;
+
+// One pass of the queue.  Field names match TileArgs where F16Tile reads
+// them.
+struct alignas(64) QPass {
+  CUtensorMap tmap_in;
+  CUtensorMap tmap_out;
+  const uint2* item_tab;
+  const uint32_t* epi_tab;
+  uint32_t lofs[16];
+  uint32_t sofs[32];
+  uint32_t kofs[kMaxStages][16];
+  const float4* tw;
+  const float2* tail_tw;
+  const float2* post_a;
+  const float2* post_b;
+  uint64_t post_mask;
+  uint32_t post_shift;
+  int inverse;
+  int32_t in_cmul[5], in_omul[5], out_cmul[5], out_omul[5];
+  int32_t in_ndims, out_ndims;
+  int64_t col_blocks;
+  uint32_t in_tile_bytes;
+  int32_t variant;      // which compiled tile routine runs this pass
+  int32_t wait_base;    // counters[wait_base + outer] >= wait_count before loading; -1: none
+  int32_t wait_count;
+  int32_t sig_base;     // after the store of tile t: +1 on counters[sig_base + k] for every
+  int32_t pad_;         //   k in [t sig_mul / sig_div, ((t + 1) sig_mul - 1) / sig_div],
+  int64_t sig_mul, sig_div, sig_kmax;  // k <= sig_kmax; sig_base -1: none
+};
+
+struct QItem {
+  uint32_t pass;
+  uint32_t tile;
+};
+
+struct alignas(64) QArgs {
+  const QItem* items;
+  int64_t nitems;
+  int* counters;
+  int* status;
+  const uint4* bmat;  // DFT-16 embedding (scaled by 1/16), 64B-swizzled K-major, 2 KB
+  int npass;
+  QPass pass[kQueueMaxPasses];
+};
+static_assert(sizeof(QArgs) <= 32764, "kernel parameter block");
+
+// Queue-kernel shared memory: the 16K-point tile buffers, then the largest
+// radix-R and stage-row tables any variant uses.
+struct QueueSmem {
+  static constexpr int STAGE_BYTES = 16384 * 4;
+  static constexpr int OFF_S0 = 0;
+  static constexpr int OFF_S1 = STAGE_BYTES;
+  static constexpr int OFF_A = 2 * STAGE_BYTES;
+  static constexpr int OFF_B = 3 * STAGE_BYTES;
+  static constexpr int OFF_TAIL = OFF_B + 2048;
+  static constexpr int OFF_TWS = OFF_TAIL + 2048 * 8;  // radix-R table of L <= 2048
+  static constexpr int OFF_BAR = OFF_TWS + 128 * 128;  // up to 128 stage rows
+  static constexpr int SMEM_BYTES = OFF_BAR + 256;     // the window base must be 1 KB aligned
+  static_assert(SMEM_BYTES <= 232448, "shared memory budget");
+};
+
+namespace queue {
+
+// Variant index of a pass: L = 32 .. 4096, with and without the four-step
+// twiddle, 16K- or 8K-point tiles (4096 only 16K);
+// variant = 16 * (8K tile) + 2 * index(L) + posttw.
+__host__ __device__ constexpr int variant_of(int L, bool posttw, int tile_points) {
+  int i = 0;
+  for (int l = 32; l < L; l <<= 1) ++i;
+  return 16 * (tile_points == 8192 ? 1 : 0) + 2 * i + (posttw ? 1 : 0);
+}
+
+}  // namespace queue
+
+// The kernel itself is compiled in one translation unit (queue.cu).
+#ifdef MCFFT_QUEUE_KERNEL
+namespace queue {
+
+__device__ __forceinline__ bool mbar_test(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}\n"
+      : "=r"(ok)
+      : "r"(sm100::smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ int ld_acquire(const int* p) {
+  int v;
+  asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void red_release_add(int* p, int v) {
+  asm volatile("red.release.gpu.global.add.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ void fence_proxy_async_global() {
+  asm volatile("fence.proxy.async.global;" ::: "memory");
+}
+
+template <int V>
+struct Variant {
+  static constexpr int LI = (V >> 1) & 7;  // L = 32 << LI
+  static constexpr int L = 32 << LI;
+  static constexpr int R = 1 << ((5 + LI) % 4);
+  static constexpr int TP = V >= 16 ? 8192 : 16384;
+  static constexpr int C = TP / L;
+  static constexpr bool PT = (V & 1) != 0;
+};
+
+// Runs this CTA's consecutive items k, k+1, ... that belong to pass `pi`
+// (whose variant is V); returns the local index of the first item of
+// another pass.  The pass's tables go to shared memory and its layout
+// entries to registers once per run.
+template <int V>
+__device__ __forceinline__ int64_t run_variant(const QArgs& a, uint32_t pi, const TileCtx& x,
+                                               uint8_t* smem, uint64_t* full, uint64_t* outrdy,
+                                               int ctid, int64_t k, int64_t nlocal,
+                                               uint32_t& mphase) {
+  using VV = Variant<V>;
+  using TL = F16Tile<VV::L, VV::R, VV::C, VV::PT, 16>;
+  static_assert(VV::C >= 4, "columns per tile");
+  const QPass& P = a.pass[pi];
+  const int64_t G = gridDim.x;
+  // every consumer is past the previous tile's last barrier, so nobody
+  // still reads the old tables
+  TL::tables(P, smem + QueueSmem::OFF_TAIL, smem + QueueSmem::OFF_TWS, ctid);
+  tile::named_bar(1, TL::NCT);
+  uint2 ient[TL::NIT_P];
+  uint32_t eent[TL::NST][TL::NIT_E];
+  TL::entries(P, ctid, ient, eent);
+  for (;;) {
+    const int b = (int)(k & 1);
+    const int64_t t = a.items[blockIdx.x + k * G].tile;
+    TL::run(P, x, ctid, b, t % P.col_blocks, mphase, ient, eent);
+    if (*x.abort_flag) return nlocal;
+    if (ctid == 0) tile::mbar_arrive(&outrdy[b]);
+    if (++k >= nlocal || a.items[blockIdx.x + k * G].pass != pi) return k;
+    if (!sm100::mbar_wait_bounded(&full[k & 1], (uint32_t)(k >> 1) & 1u, kWaitLimit)) {
+      *x.abort_flag = 1;
+      return nlocal;
+    }
+    if (*x.abort_flag) return nlocal;
+  }
+}
+
+}  // namespace queue
+
+// 16 consumer warps + 1 producer warp; 96 registers (17 warps are granted
+// registers as 20).
+__global__ void __maxnreg__(96) fft_queue_f16(const __grid_constant__ QArgs a) {
+  constexpr int NCW = 16, NCT = NCW * 32, NMT = 8, TMEM_COLS = 256;
+  using Q = QueueSmem;
+  extern __shared__ uint8_t smem[];
+  const uint32_t base_u = sm100::smem_u32(smem);
+  const uint32_t sS0 = base_u + Q::OFF_S0, sS1 = base_u + Q::OFF_S1, sA = base_u + Q::OFF_A;
+  const uint32_t bS0 = sS0 - kWinBase, bS1 = sS1 - kWinBase, bA = sA - kWinBase;
+  if ((base_u & 1023u) != 0 || ((bS0 | bS1 | bA) & (uint32_t)(Q::STAGE_BYTES - 1)) != 0) {
+    if (threadIdx.x == 0 && a.status) atomicExch(a.status, kStatusLayout);
+    return;
+  }
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + Q::OFF_BAR);  // [2]
+  uint64_t* outrdy = full + 2;                                      // [2]
+  uint64_t* mmab = full + 4;                                        // [NMT]
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(full + 4 + 16);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(full + 4 + 17);
+  const int tid = threadIdx.x;
+  const int warp = tid >> 5, lane = tid & 31;
+  const bool producer = warp == NCW;
+  const int64_t G = gridDim.x;
+  const int64_t nlocal = a.nitems > blockIdx.x ? (a.nitems - blockIdx.x + G - 1) / G : 0;
+
+  if (producer) {
+    if (lane == 0) {
+      sm100::mbar_init(&full[0], 1);
+      sm100::mbar_init(&full[1], 1);
+      sm100::mbar_init(&outrdy[0], 1);
+      sm100::mbar_init(&outrdy[1], 1);
+      for (int m = 0; m < NMT; ++m) sm100::mbar_init(&mmab[m], 1);
+      *abort_flag = 0;
+      sm100::fence_mbar_init();
+    }
+    __syncwarp();
+    sm100::tmem_alloc(tmem_slot, TMEM_COLS);
+    sm100::tmem_relinquish();
+  } else {
+    for (int i = tid; i < 128; i += NCT)
+      *reinterpret_cast<uint4*>(smem + Q::OFF_B + 16 * i) = __ldg(a.bmat + i);
+  }
+  sm100::fence_proxy_async_smem();
+  sm100::tc_fence_before();
+  __syncthreads();
+  sm100::tc_fence_after();
+  const uint32_t tmem_base = *tmem_slot;
+  const TileCtx x{sS0, sS1, sA, base_u + Q::OFF_B, base_u + Q::OFF_TAIL, base_u + Q::OFF_TWS,
+                  bS0, bS1, bA, tmem_base, mmab, abort_flag};
+
+  if (producer) {
+    // ------------------------------------------------------------- producer
+    // Event loop: store finished tiles as soon as the consumers release
+    // them; load the next tile once its buffer is free and its dependency
+    // is met.  Never blocks on one while the other could proceed.
+    if (lane == 0) {
+      int64_t il = 0, is = 0;  // next local item to load / to store
+      int64_t sig = -1;        // stored item whose completion is still to be signalled
+      uint32_t idle = 0;
+      // Completion of a producing tile: its bulk store has finished writing,
+      // then a release add on every key it covers.
+      auto signal = [&](int64_t k) {
+        const QItem it = a.items[blockIdx.x + k * G];
+        const QPass& P = a.pass[it.pass];
+        tile::tma_store_wait_all();
+        queue::fence_proxy_async_global();
+        const int64_t k0 = (int64_t)it.tile * P.sig_mul / P.sig_div;
+        int64_t k1 = ((int64_t)it.tile * P.sig_mul + P.sig_mul - 1) / P.sig_div;
+        if (k1 > P.sig_kmax) k1 = P.sig_kmax;
+        for (int64_t key = k0; key <= k1; ++key)
+          queue::red_release_add(a.counters + P.sig_base + key, 1);
+      };
+      while (is < nlocal) {
+        bool moved = false;
+        if (is < il && queue::mbar_test(&outrdy[is & 1], (uint32_t)(is >> 1) & 1u)) {
+          const QItem it = a.items[blockIdx.x + is * G];
+          const QPass& P = a.pass[it.pass];
+          int32_t crd[5];
+          tile::tile_coords(P.out_cmul, P.out_omul, it.tile % P.col_blocks, it.tile / P.col_blocks, crd);
+          tile::tma_store(&P.tmap_out, P.out_ndims, crd, (is & 1) ? sS1 : sS0);
+          tile::tma_store_wait_read();
+          if (sig >= 0) signal(sig);
+          sig = P.sig_base >= 0 ? is : -1;
+          ++is;
+          moved = true;
+        }
+        if (il < nlocal && il < is + 2 && !*abort_flag) {
+          const QItem it = a.items[blockIdx.x + il * G];
+          const QPass& P = a.pass[it.pass];
+          const int64_t outer = it.tile / P.col_blocks;
+          bool ready = true;
+          if (P.wait_base >= 0) {
+            ready = queue::ld_acquire(a.counters + P.wait_base + outer) >= P.wait_count;
+            if (ready) queue::fence_proxy_async_global();
+          }
+          if (ready) {
+            int32_t crd[5];
+            tile::tile_coords(P.in_cmul, P.in_omul, it.tile % P.col_blocks, outer, crd);
+            sm100::mbar_arrive_expect_tx(&full[il & 1], P.in_tile_bytes);
+            tile::tma_load(&P.tmap_in, P.in_ndims, crd, (il & 1) ? sS1 : sS0, &full[il & 1]);
+            ++il;
+            moved = true;
+          }
+        }
+        // Signal after the attempt to issue the next load, so that waiting
+        // for the store's completion does not delay it (and never later: the
+        // next load may depend on this very tile).
+        if (sig >= 0) {
+          signal(sig);
+          sig = -1;
+        }
+        if (moved) {
+          idle = 0;
+        } else {
+          if (*abort_flag || ++idle > kWaitLimit) {
+            *abort_flag = 1;
+            break;
+          }
+          __nanosleep(32);
+        }
+      }
+      if (sig >= 0) signal(sig);
+      tile::tma_store_wait_all();
+      // Loads issued but not consumed (abort path) must land before the
+      // CTA's shared memory is released.
+      for (int64_t k = is; k < il; ++k)
+        sm100::mbar_wait_bounded(&full[k & 1], (uint32_t)(k >> 1) & 1u, kWaitLimit);
+    }
+    __syncwarp();
+  } else {
+    // ------------------------------------------------------------ consumers
+    uint32_t mphase = 0;  // bit m: phase of mmab[m] (variants use 4 or 8 M-tiles)
+    for (int64_t k = 0; k < nlocal;) {
+      if (!sm100::mbar_wait_bounded(&full[k & 1], (uint32_t)(k >> 1) & 1u, kWaitLimit)) *abort_flag = 1;
+      if (*abort_flag) break;
+      const uint32_t pi = a.items[blockIdx.x + k * G].pass;
+      switch (a.pass[pi].variant) {
+#define MCFFT_QCASE(V)                                                                   \
+  case V:                                                                                \
+    k = queue::run_variant<V>(a, pi, x, smem, full, outrdy, tid, k, nlocal, mphase); \
+    break;
+        MCFFT_QCASE(0) MCFFT_QCASE(1) MCFFT_QCASE(2) MCFFT_QCASE(3)
+        MCFFT_QCASE(16) MCFFT_QCASE(17)
+        MCFFT_QCASE(4) MCFFT_QCASE(5) MCFFT_QCASE(6) MCFFT_QCASE(7)
+        MCFFT_QCASE(8) MCFFT_QCASE(9) MCFFT_QCASE(10) MCFFT_QCASE(11)
+        MCFFT_QCASE(12) MCFFT_QCASE(13) MCFFT_QCASE(14) MCFFT_QCASE(15)
+        MCFFT_QCASE(18) MCFFT_QCASE(19) MCFFT_QCASE(20) MCFFT_QCASE(21)
+        MCFFT_QCASE(22) MCFFT_QCASE(23) MCFFT_QCASE(24) MCFFT_QCASE(25)
+        MCFFT_QCASE(26) MCFFT_QCASE(27) MCFFT_QCASE(28) MCFFT_QCASE(29)
+#undef MCFFT_QCASE
+        default: *abort_flag = 1; break;
+      }
+      if (*abort_flag) break;
+    }
+  }
+  __syncthreads();
+  if (tid == 0 && *abort_flag && a.status) atomicExch(a.status, kStatusTimeout);
+  if (producer) sm100::tmem_dealloc(tmem_base, TMEM_COLS);
+}
+
+#endif  // MCFFT_QUEUE_KERNEL
+
+}  // namespace mcfft

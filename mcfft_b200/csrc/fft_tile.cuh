@@ -349,17 +349,29 @@ __device__ __forceinline__ void small_dft_h2(__half2 (&x)[R], float sgn) {
   }
 }
 
+// Per-CTA shared-memory and tensor-memory handles of the tile routines.
+struct TileCtx {
+  uint32_t sS0, sS1, sA, sB, sTail, sTws;  // shared addresses
+  uint32_t bS0, bS1, bA;                   // the same, relative to the window base
+  uint32_t tmem;                           // TMEM accumulator base
+  uint64_t* mmab;                          // per-M-tile MMA completion barriers
+  volatile int* abort_flag;
+};
+
+// One tile of one pass, plain FP16 form: prologue, radix-16 stages on
+// tcgen05 and their epilogues, run by the NCW consumer warps once the
+// tile's staging buffer b holds its input.  `A` is any argument block with
+// the pass's layout tables and twiddle pointers (the per-pass kernel's
+// TileArgs, or one pass of the batch queue).
 template <int L, int R, int C, bool POSTTW, int NCW>
-// Registers are granted per block in units of four warps: 17 warps (16
-// consumers + producer) count as 20, so 65536 / 640 -> 96 per thread; the
-// 9-warp variants count as 12 warps and run two CTAs per SM -> 80.
-__global__ void __maxnreg__(NCW <= 8 ? 80 : 96) fft_tile_f16(const __grid_constant__ TileArgs a) {
+struct F16Tile {
   using S = TileShape<L, R, C, NCW>;
   using T = TileF16<L, R, C, POSTTW, NCW>;
-  constexpr int NCT = S::NCT;
-  constexpr int NIT_P = (S::ITEMS + NCT - 1) / NCT;  // prologue items per consumer thread
-  constexpr int NIT_E = S::NMT * 4 / NCW;            // 32-row blocks per warp per stage
-  constexpr int NMT = S::NMT;
+  static constexpr int NCT = S::NCT;
+  static constexpr int NIT_P = (S::ITEMS + NCT - 1) / NCT;  // prologue items per consumer thread
+  static constexpr int NIT_E = S::NMT * 4 / NCW;            // 32-row blocks per warp per stage
+  static constexpr int NMT = S::NMT;
+  static constexpr int NST = S::NST;
   static_assert(S::NMT * 4 % NCW == 0, "row blocks per warp");
   static_assert(NMT <= 16, "per-M-tile barriers");
   // Operand buffers alternate between the A buffer and the tile's staging
@@ -367,7 +379,255 @@ __global__ void __maxnreg__(NCW <= 8 ? 80 : 96) fft_tile_f16(const __grid_consta
   // read, and the last stage writes the staging buffer (the TMA store
   // source).  X[s] = A when NST - s is odd, staging otherwise; with an even
   // stage count the prologue transposes the staging buffer in place.
-  constexpr bool INPLACE_PROLOGUE = (S::NST % 2) == 0;
+  static constexpr bool INPLACE_PROLOGUE = (S::NST % 2) == 0;
+
+  // This thread's prologue items and epilogue rows (the same for every tile
+  // of a pass).
+  template <class A>
+  static __device__ __forceinline__ void entries(const A& a, int ctid, uint2 (&ient)[NIT_P],
+                                                 uint32_t (&eent)[NST][NIT_E]) {
+    const int warp = ctid >> 5, lane = ctid & 31, sp = warp & 3;
+#pragma unroll
+    for (int j = 0; j < NIT_P; ++j) {
+      const int it = ctid + j * NCT;
+      ient[j] = it < S::ITEMS ? __ldg(a.item_tab + it) : make_uint2(0u, 0u);
+    }
+#pragma unroll
+    for (int s = 0; s < NST; ++s)
+#pragma unroll
+      for (int j = 0; j < NIT_E; ++j) {
+        const uint32_t m = (warp >> 2) + j * (NCW / 4);
+        eent[s][j] = __ldg(a.epi_tab + s * S::NROWS + m * 128 + sp * 32 + lane);
+      }
+  }
+
+  // Radix-R twiddles (as packed-FP16 pairs {(wr, wr), (-wi, wi)}) and stage
+  // twiddle rows into shared memory; consumer threads only.
+  template <class A>
+  static __device__ __forceinline__ void tables(const A& a, uint8_t* tail, uint8_t* tws, int ctid) {
+    if constexpr (R > 1) {
+      for (int i = ctid; i < L; i += NCT) {
+        const float2 w = __ldg(a.tail_tw + i);
+        const __half2 wrr = __float2half2_rn(w.x);
+        const __half2 wni = __floats2half2_rn(-w.y, w.y);
+        uint2 v;
+        v.x = *reinterpret_cast<const uint32_t*>(&wrr);
+        v.y = *reinterpret_cast<const uint32_t*>(&wni);
+        *reinterpret_cast<uint2*>(tail + 8 * i) = v;
+      }
+    }
+    if constexpr (T::TW_SMEM && T::TW_ROWS > 0) {
+      for (int i = ctid; i < T::TW_ROWS * 8; i += NCT)
+        *reinterpret_cast<float4*>(tws + 16 * i) = __ldg(a.tw + i);
+    }
+  }
+
+  template <class A>
+  static __device__ __forceinline__ void run(const A& a, const TileCtx& x, int ctid, int b,
+                                             int64_t cb, uint32_t& mphase,  // bit m: phase of mmab[m]
+                                             const uint2 (&ient)[NIT_P],
+                                             const uint32_t (&eent)[NST][NIT_E]) {
+    const int warp = ctid >> 5, lane = ctid & 31, sp = warp & 3;
+    constexpr uint32_t IDESC = sm100::idesc_f16_f32(128, 32);
+    const float tsgn = a.inverse ? 1.f : -1.f;
+    const uint32_t sb = b ? x.sS1 : x.sS0;
+    // ---------------------------------------------------------- prologue
+    // Offsets are XOR-linear relative to their buffer.
+    const uint32_t bb = b ? x.bS1 : x.bS0;
+    const uint32_t x0 = INPLACE_PROLOGUE ? bb : x.bA;  // stage-0 operand buffer
+    if constexpr (R == 1) {
+      uint4 q[NIT_P][4];
+#pragma unroll
+      for (int j = 0; j < NIT_P; ++j) {
+        const uint32_t lb = (ient[j].x & 0xFFFFu) << 2;
+#pragma unroll
+        for (int n = 0; n < 4; ++n) q[j][n] = lds128w(xo(lb, a.lofs[n], bb));
+      }
+      if (INPLACE_PROLOGUE) tile::named_bar(1, NCT);
+#pragma unroll
+      for (int j = 0; j < NIT_P; ++j) {
+        if (S::ITEMS % NCT != 0 && ctid + j * NCT >= S::ITEMS) break;
+        const uint32_t st = (ient[j].x >> 16) << 2;
+        sts128w(xo(st, a.sofs[0], x0), make_uint4(q[j][0].x, q[j][1].x, q[j][2].x, q[j][3].x));
+        sts128w(xo(st, a.sofs[1], x0), make_uint4(q[j][0].y, q[j][1].y, q[j][2].y, q[j][3].y));
+        sts128w(xo(st, a.sofs[2], x0), make_uint4(q[j][0].z, q[j][1].z, q[j][2].z, q[j][3].z));
+        sts128w(xo(st, a.sofs[3], x0), make_uint4(q[j][0].w, q[j][1].w, q[j][2].w, q[j][3].w));
+      }
+    } else {
+      uint4 q[NIT_P][R];
+#pragma unroll
+      for (int j = 0; j < NIT_P; ++j) {
+        const uint32_t lb = (ient[j].x & 0xFFFFu) << 2;
+#pragma unroll
+        for (int n = 0; n < R; ++n) q[j][n] = lds128w(xo(lb, a.lofs[n], bb));
+      }
+      if (INPLACE_PROLOGUE) tile::named_bar(1, NCT);
+#pragma unroll
+      for (int j = 0; j < NIT_P; ++j) {
+        if (S::ITEMS % NCT != 0 && ctid + j * NCT >= S::ITEMS) break;
+        const uint32_t st = (ient[j].x >> 16) << 2;
+        // item word 1: tail twiddle row of sub-vector 0; bit 31 set for
+        // column items (all four sub-vectors share the row)
+        const uint32_t trow = ient[j].y & 0x7FFFFFFFu;
+        const bool colitem = (ient[j].y >> 31) != 0;
+#pragma unroll
+        for (int jj = 0; jj < 4; ++jj) {
+          __half2 hv[R];
+#pragma unroll
+          for (int n = 0; n < R; ++n) {
+            const uint32_t w = jj == 0 ? q[j][n].x : jj == 1 ? q[j][n].y : jj == 2 ? q[j][n].z : q[j][n].w;
+            hv[n] = *reinterpret_cast<const __half2*>(&w);
+          }
+          small_dft_h2<R>(hv, tsgn);
+          const uint32_t vr = colitem ? trow : trow + jj;
+          const uint32_t twa = x.sTail + vr * (R * 8);
+#pragma unroll
+          for (int k2 = 0; k2 < R / 2; ++k2) {
+            const uint4 tw = tile::lds128(twa + 16 * k2);
+            const __half2 y0 = h2cmul(hv[2 * k2], *reinterpret_cast<const __half2*>(&tw.x),
+                                      *reinterpret_cast<const __half2*>(&tw.y));
+            const __half2 y1 = h2cmul(hv[2 * k2 + 1], *reinterpret_cast<const __half2*>(&tw.z),
+                                      *reinterpret_cast<const __half2*>(&tw.w));
+            sts32w(xo(st, a.sofs[jj * R + 2 * k2], x0), *reinterpret_cast<const uint32_t*>(&y0));
+            sts32w(xo(st, a.sofs[jj * R + 2 * k2 + 1], x0), *reinterpret_cast<const uint32_t*>(&y1));
+          }
+        }
+      }
+    }
+    sm100::fence_proxy_async_smem();
+    sm100::tc_fence_before();
+    tile::named_bar(1, NCT);
+    sm100::tc_fence_after();
+
+    // ------------------------------------------------------------ stages
+#pragma unroll
+    for (int s = 0; s < S::NST; ++s) {
+      const uint32_t xs = ((S::NST - s) & 1) ? x.sA : sb;       // this stage's operand
+      const uint32_t xn = ((S::NST - s) & 1) ? bb : x.bA;       // next stage's operand (window-relative)
+      // Each M-tile's two MMAs and its commit are issued by lane 0 of the
+      // sub-partition-0 warp that drains that M-tile, so four warps issue
+      // in parallel (a single issuing thread serialises ~100 cycles per
+      // tcgen05.mma).  tcgen05.commit tracks the issuing thread's MMAs.
+      if (sp == 0 && lane == 0) {
+#pragma unroll
+        for (int j = 0; j < NIT_E; ++j) {
+          const uint32_t m = (warp >> 2) + j * (NCW / 4);
+#pragma unroll
+          for (int ks = 0; ks < 2; ++ks)
+            sm100::umma_f16(x.tmem + 32u * m, tile::sdesc_sw64(xs + m * 8192u + ks * 32u),
+                            tile::sdesc_sw64(x.sB + ks * 32u), IDESC, ks);
+          sm100::umma_commit(&x.mmab[m]);
+        }
+      }
+      const bool last = s == S::NST - 1;
+      const uint32_t row0 = stage_tw_row0<L, R>(s);
+#pragma unroll
+      for (int j = 0; j < NIT_E; ++j) {
+        const uint32_t m = (warp >> 2) + j * (NCW / 4);
+        const uint32_t e = eent[s][j];
+        const uint32_t aux = e >> 16;
+        const uint32_t dst = (e & 0xFFFFu) << 2;
+        // TMEM columns per lane (the DFT-16 matrix's N order): for point
+        // pair p, d[4p..4p+3] = (re_2p, re_2p+1, im_2p, im_2p+1).  The 1/16
+        // stage scale is in the matrix.
+        float4 wg[8];
+        if (!last && !T::TW_SMEM) {
+          const float4* t4 = a.tw + (size_t)(row0 + aux) * 8;
+#pragma unroll
+          for (int p = 0; p < 8; ++p) wg[p] = __ldg(t4 + (p ^ tw_fold(aux)));
+        }
+        if (!sm100::mbar_wait_bounded(&x.mmab[m], (mphase >> m) & 1u, kWaitLimit)) *x.abort_flag = 1;
+        sm100::tc_fence_after();
+        uint32_t d[32];
+        sm100::tmem_ld32(x.tmem + ((uint32_t)(32 * sp) << 16) + 32u * m, d);
+        if (!last) {
+          const uint32_t trow = x.sTws + (row0 + aux) * 128u;
+          const uint32_t fold = tw_fold(aux);
+          sm100::tmem_wait_ld();
+#pragma unroll
+          for (int h = 0; h < 2; ++h) {
+            float4 w[4];
+#pragma unroll
+            for (int pp = 0; pp < 4; ++pp)
+              w[pp] = T::TW_SMEM ? lds128f(trow + (((4 * h + pp) ^ fold) << 4)) : wg[4 * h + pp];
+#pragma unroll
+            for (int pp = 0; pp < 4; ++pp) {
+              const int p = 4 * h + pp;
+              uint64_t yr, yi;
+              cmul2(f2p(__uint_as_float(d[4 * p]), __uint_as_float(d[4 * p + 1])),
+                    f2p(__uint_as_float(d[4 * p + 2]), __uint_as_float(d[4 * p + 3])),
+                    f2p(w[pp].x, w[pp].y), f2p(w[pp].z, w[pp].w), yr, yi);
+              float r0, r1, i0, i1;
+              f2u(yr, r0, r1);
+              f2u(yi, i0, i1);
+              sts32w(xo(dst, a.kofs[s][2 * p], xn), sm100::pack_half2(r0, i0));
+              sts32w(xo(dst, a.kofs[s][2 * p + 1], xn), sm100::pack_half2(r1, i1));
+            }
+          }
+        } else if (POSTTW) {
+          // Four-step twiddle W_N^((v + NV k) g): pairs (w_2p, w_2p+1)
+          // from w_0 = W_N^(v g) and ws = W_N^(NV g), advanced by ws^2
+          // (FP32 recurrence, 7 steps, far below the FP16 output rounding).
+          const uint32_t v = aux / C, c = aux % C;
+          const uint64_t g = (uint64_t)(cb * C + c);
+          const uint64_t e0 = ((uint64_t)v * g) & a.post_mask;
+          const uint64_t es = ((uint64_t)S::NV * g) & a.post_mask;
+          const float2 w0 = twiddle2(a.post_a, a.post_b, e0, a.post_shift);
+          const float2 ws = twiddle2(a.post_a, a.post_b, es, a.post_shift);
+          const float2 w1 = cmulf(w0, ws);
+          const float2 s2 = cmulf(ws, ws);
+          uint64_t wr = f2p(w0.x, w1.x), wi = f2p(w0.y, w1.y);
+          const uint64_t s2r = f2p(s2.x, s2.x), s2i = f2p(s2.y, s2.y);
+          sm100::tmem_wait_ld();
+#pragma unroll
+          for (int p = 0; p < 8; ++p) {
+            uint64_t yr, yi;
+            cmul2(f2p(__uint_as_float(d[4 * p]), __uint_as_float(d[4 * p + 1])),
+                  f2p(__uint_as_float(d[4 * p + 2]), __uint_as_float(d[4 * p + 3])), wr, wi, yr,
+                  yi);
+            float r0, r1, i0, i1;
+            f2u(yr, r0, r1);
+            f2u(yi, i0, i1);
+            sts32w(xo(dst, a.kofs[s][2 * p], bb), sm100::pack_half2(r0, i0));
+            sts32w(xo(dst, a.kofs[s][2 * p + 1], bb), sm100::pack_half2(r1, i1));
+            if (p < 7) {
+              uint64_t nr, ni;
+              cmul2(wr, wi, s2r, s2i, nr, ni);
+              wr = nr;
+              wi = ni;
+            }
+          }
+        } else {
+          sm100::tmem_wait_ld();
+#pragma unroll
+          for (int p = 0; p < 8; ++p) {
+            sts32w(xo(dst, a.kofs[s][2 * p], bb),
+                   sm100::pack_half2(__uint_as_float(d[4 * p]), __uint_as_float(d[4 * p + 2])));
+            sts32w(xo(dst, a.kofs[s][2 * p + 1], bb),
+                   sm100::pack_half2(__uint_as_float(d[4 * p + 1]), __uint_as_float(d[4 * p + 3])));
+          }
+        }
+      }
+      mphase ^= (1u << NMT) - 1u;
+      sm100::fence_proxy_async_smem();
+      sm100::tc_fence_before();
+      tile::named_bar(1, NCT);
+      sm100::tc_fence_after();
+      if (*x.abort_flag) break;
+    }
+  }
+};
+
+template <int L, int R, int C, bool POSTTW, int NCW>
+// Registers are granted per block in units of four warps: 17 warps (16
+// consumers + producer) count as 20, so 65536 / 640 -> 96 per thread; the
+// 9-warp variants count as 12 warps and run two CTAs per SM -> 80.
+__global__ void __maxnreg__(NCW <= 8 ? 80 : 96) fft_tile_f16(const __grid_constant__ TileArgs a) {
+  using S = TileShape<L, R, C, NCW>;
+  using T = TileF16<L, R, C, POSTTW, NCW>;
+  using TL = F16Tile<L, R, C, POSTTW, NCW>;
+  constexpr int NCT = S::NCT;
+  constexpr int NMT = S::NMT;
   extern __shared__ uint8_t smem_raw[];
   const uint32_t raw_u = sm100::smem_u32(smem_raw);
   const uint32_t base_u = (raw_u + 1023u) & ~1023u;
@@ -410,28 +670,14 @@ __global__ void __maxnreg__(NCW <= 8 ? 80 : 96) fft_tile_f16(const __grid_consta
   } else {
     for (int i = tid; i < 128; i += NCT)
       *reinterpret_cast<uint4*>(smem + T::OFF_B + 16 * i) = __ldg(a.bmat + i);
-    if constexpr (R > 1) {
-      // radix-R twiddles as packed-FP16 pairs {(wr, wr), (-wi, wi)}
-      for (int i = tid; i < L; i += NCT) {
-        const float2 w = __ldg(a.tail_tw + i);
-        const __half2 wrr = __float2half2_rn(w.x);
-        const __half2 wni = __floats2half2_rn(-w.y, w.y);
-        uint2 v;
-        v.x = *reinterpret_cast<const uint32_t*>(&wrr);
-        v.y = *reinterpret_cast<const uint32_t*>(&wni);
-        *reinterpret_cast<uint2*>(smem + T::OFF_TAIL + 8 * i) = v;
-      }
-    }
-    if constexpr (T::TW_SMEM && T::TW_ROWS > 0) {
-      for (int i = tid; i < T::TW_ROWS * 8; i += NCT)
-        *reinterpret_cast<float4*>(smem + T::OFF_TWS + 16 * i) = __ldg(a.tw + i);
-    }
+    TL::tables(a, smem + T::OFF_TAIL, smem + T::OFF_TWS, tid);
   }
   sm100::fence_proxy_async_smem();
   sm100::tc_fence_before();
   __syncthreads();
   sm100::tc_fence_after();
   const uint32_t tmem_base = *tmem_slot;
+  const TileCtx x{sS0, sS1, sA, sB, sTail, sTws, bS0, bS1, bA, tmem_base, mmab, abort_flag};
 
   if (producer) {
     // ------------------------------------------------------------- producer
@@ -480,223 +726,20 @@ __global__ void __maxnreg__(NCW <= 8 ? 80 : 96) fft_tile_f16(const __grid_consta
     __syncwarp();
   } else {
     // ------------------------------------------------------------ consumers
-    const int ctid = tid;  // 0 .. NCT-1
-    const int sp = warp & 3;
-    constexpr uint32_t IDESC = sm100::idesc_f16_f32(128, 32);
-    uint32_t mphase = 0;  // completions of every per-M-tile barrier so far, mod 2
-    const float tsgn = a.inverse ? 1.f : -1.f;
-
     // The tables are the same for every tile: keep this thread's entries in
     // registers for the whole launch.
-    uint2 ient[NIT_P];
-#pragma unroll
-    for (int j = 0; j < NIT_P; ++j) {
-      const int it = ctid + j * NCT;
-      ient[j] = it < S::ITEMS ? __ldg(a.item_tab + it) : make_uint2(0u, 0u);
-    }
-    uint32_t eent[S::NST][NIT_E];
-#pragma unroll
-    for (int s = 0; s < S::NST; ++s)
-#pragma unroll
-      for (int j = 0; j < NIT_E; ++j) {
-        const uint32_t m = (warp >> 2) + j * (NCW / 4);
-        eent[s][j] = __ldg(a.epi_tab + s * S::NROWS + m * 128 + sp * 32 + lane);
-      }
-
+    uint2 ient[TL::NIT_P];
+    uint32_t eent[TL::NST][TL::NIT_E];
+    TL::entries(a, tid, ient, eent);
+    uint32_t mphase = 0;  // bit m: completions of M-tile barrier m so far, mod 2
     int i = 0;
     for (int64_t t = blockIdx.x; t < a.ntiles; t += gridDim.x, ++i) {
       const int b = i & 1;
-      const uint32_t sb = b ? sS1 : sS0;
-      const int64_t cb = t % a.col_blocks;
       if (!sm100::mbar_wait_bounded(&full[b], (i >> 1) & 1, kWaitLimit)) *abort_flag = 1;
       if (*abort_flag) break;
-
-      // ---------------------------------------------------------- prologue
-      // Offsets are XOR-linear relative to their buffer.
-      const uint32_t bb = b ? bS1 : bS0;
-      const uint32_t x0 = INPLACE_PROLOGUE ? bb : bA;  // stage-0 operand buffer
-      if constexpr (R == 1) {
-        uint4 q[NIT_P][4];
-#pragma unroll
-        for (int j = 0; j < NIT_P; ++j) {
-          const uint32_t lb = (ient[j].x & 0xFFFFu) << 2;
-#pragma unroll
-          for (int n = 0; n < 4; ++n) q[j][n] = lds128w(xo(lb, a.lofs[n], bb));
-        }
-        if (INPLACE_PROLOGUE) tile::named_bar(1, NCT);
-#pragma unroll
-        for (int j = 0; j < NIT_P; ++j) {
-          if (S::ITEMS % NCT != 0 && ctid + j * NCT >= S::ITEMS) break;
-          const uint32_t st = (ient[j].x >> 16) << 2;
-          sts128w(xo(st, a.sofs[0], x0), make_uint4(q[j][0].x, q[j][1].x, q[j][2].x, q[j][3].x));
-          sts128w(xo(st, a.sofs[1], x0), make_uint4(q[j][0].y, q[j][1].y, q[j][2].y, q[j][3].y));
-          sts128w(xo(st, a.sofs[2], x0), make_uint4(q[j][0].z, q[j][1].z, q[j][2].z, q[j][3].z));
-          sts128w(xo(st, a.sofs[3], x0), make_uint4(q[j][0].w, q[j][1].w, q[j][2].w, q[j][3].w));
-        }
-      } else {
-        uint4 q[NIT_P][R];
-#pragma unroll
-        for (int j = 0; j < NIT_P; ++j) {
-          const uint32_t lb = (ient[j].x & 0xFFFFu) << 2;
-#pragma unroll
-          for (int n = 0; n < R; ++n) q[j][n] = lds128w(xo(lb, a.lofs[n], bb));
-        }
-        if (INPLACE_PROLOGUE) tile::named_bar(1, NCT);
-#pragma unroll
-        for (int j = 0; j < NIT_P; ++j) {
-          if (S::ITEMS % NCT != 0 && ctid + j * NCT >= S::ITEMS) break;
-          const uint32_t st = (ient[j].x >> 16) << 2;
-          // item word 1: tail twiddle row of sub-vector 0; bit 31 set for
-          // column items (all four sub-vectors share the row)
-          const uint32_t trow = ient[j].y & 0x7FFFFFFFu;
-          const bool colitem = (ient[j].y >> 31) != 0;
-#pragma unroll
-          for (int jj = 0; jj < 4; ++jj) {
-            __half2 x[R];
-#pragma unroll
-            for (int n = 0; n < R; ++n) {
-              const uint32_t w = jj == 0 ? q[j][n].x : jj == 1 ? q[j][n].y : jj == 2 ? q[j][n].z : q[j][n].w;
-              x[n] = *reinterpret_cast<const __half2*>(&w);
-            }
-            small_dft_h2<R>(x, tsgn);
-            const uint32_t vr = colitem ? trow : trow + jj;
-            const uint32_t twa = sTail + vr * (R * 8);
-#pragma unroll
-            for (int k2 = 0; k2 < R / 2; ++k2) {
-              const uint4 tw = tile::lds128(twa + 16 * k2);
-              const __half2 y0 = h2cmul(x[2 * k2], *reinterpret_cast<const __half2*>(&tw.x),
-                                        *reinterpret_cast<const __half2*>(&tw.y));
-              const __half2 y1 = h2cmul(x[2 * k2 + 1], *reinterpret_cast<const __half2*>(&tw.z),
-                                        *reinterpret_cast<const __half2*>(&tw.w));
-              sts32w(xo(st, a.sofs[jj * R + 2 * k2], x0), *reinterpret_cast<const uint32_t*>(&y0));
-              sts32w(xo(st, a.sofs[jj * R + 2 * k2 + 1], x0), *reinterpret_cast<const uint32_t*>(&y1));
-            }
-          }
-        }
-      }
-      sm100::fence_proxy_async_smem();
-      sm100::tc_fence_before();
-      tile::named_bar(1, NCT);
-      sm100::tc_fence_after();
-
-      // ------------------------------------------------------------ stages
-#pragma unroll
-      for (int s = 0; s < S::NST; ++s) {
-        const uint32_t xs = ((S::NST - s) & 1) ? sA : sb;       // this stage's operand
-        const uint32_t xn = ((S::NST - s) & 1) ? bb : bA;       // next stage's operand (window-relative)
-        // Each M-tile's two MMAs and its commit are issued by lane 0 of the
-        // sub-partition-0 warp that drains that M-tile, so four warps issue
-        // in parallel (a single issuing thread serialises ~100 cycles per
-        // tcgen05.mma).  tcgen05.commit tracks the issuing thread's MMAs.
-        if (sp == 0 && lane == 0) {
-#pragma unroll
-          for (int j = 0; j < NIT_E; ++j) {
-            const uint32_t m = (warp >> 2) + j * (NCW / 4);
-#pragma unroll
-            for (int ks = 0; ks < 2; ++ks)
-              sm100::umma_f16(tmem_base + 32u * m, tile::sdesc_sw64(xs + m * 8192u + ks * 32u),
-                              tile::sdesc_sw64(sB + ks * 32u), IDESC, ks);
-            sm100::umma_commit(&mmab[m]);
-          }
-        }
-        const bool last = s == S::NST - 1;
-        const uint32_t row0 = stage_tw_row0<L, R>(s);
-#pragma unroll
-        for (int j = 0; j < NIT_E; ++j) {
-          const uint32_t m = (warp >> 2) + j * (NCW / 4);
-          const uint32_t e = eent[s][j];
-          const uint32_t aux = e >> 16;
-          const uint32_t dst = (e & 0xFFFFu) << 2;
-          // TMEM columns per lane (the DFT-16 matrix's N order): for point
-          // pair p, d[4p..4p+3] = (re_2p, re_2p+1, im_2p, im_2p+1).  The 1/16
-          // stage scale is in the matrix.
-          float4 wg[8];
-          if (!last && !T::TW_SMEM) {
-            const float4* t4 = a.tw + (size_t)(row0 + aux) * 8;
-#pragma unroll
-            for (int p = 0; p < 8; ++p) wg[p] = __ldg(t4 + (p ^ tw_fold(aux)));
-          }
-          if (!sm100::mbar_wait_bounded(&mmab[m], mphase, kWaitLimit)) *abort_flag = 1;
-          sm100::tc_fence_after();
-          uint32_t d[32];
-          sm100::tmem_ld32(tmem_base + ((uint32_t)(32 * sp) << 16) + 32u * m, d);
-          if (!last) {
-            const uint32_t trow = sTws + (row0 + aux) * 128u;
-            const uint32_t fold = tw_fold(aux);
-            sm100::tmem_wait_ld();
-#pragma unroll
-            for (int h = 0; h < 2; ++h) {
-              float4 w[4];
-#pragma unroll
-              for (int pp = 0; pp < 4; ++pp)
-                w[pp] = T::TW_SMEM ? lds128f(trow + (((4 * h + pp) ^ fold) << 4)) : wg[4 * h + pp];
-#pragma unroll
-              for (int pp = 0; pp < 4; ++pp) {
-                const int p = 4 * h + pp;
-                uint64_t yr, yi;
-                cmul2(f2p(__uint_as_float(d[4 * p]), __uint_as_float(d[4 * p + 1])),
-                      f2p(__uint_as_float(d[4 * p + 2]), __uint_as_float(d[4 * p + 3])),
-                      f2p(w[pp].x, w[pp].y), f2p(w[pp].z, w[pp].w), yr, yi);
-                float r0, r1, i0, i1;
-                f2u(yr, r0, r1);
-                f2u(yi, i0, i1);
-                sts32w(xo(dst, a.kofs[s][2 * p], xn), sm100::pack_half2(r0, i0));
-                sts32w(xo(dst, a.kofs[s][2 * p + 1], xn), sm100::pack_half2(r1, i1));
-              }
-            }
-          } else if (POSTTW) {
-            // Four-step twiddle W_N^((v + NV k) g): pairs (w_2p, w_2p+1)
-            // from w_0 = W_N^(v g) and ws = W_N^(NV g), advanced by ws^2
-            // (FP32 recurrence, 7 steps, far below the FP16 output rounding).
-            const uint32_t v = aux / C, c = aux % C;
-            const uint64_t g = (uint64_t)(cb * C + c);
-            const uint64_t e0 = ((uint64_t)v * g) & a.post_mask;
-            const uint64_t es = ((uint64_t)S::NV * g) & a.post_mask;
-            const float2 w0 = twiddle2(a.post_a, a.post_b, e0, a.post_shift);
-            const float2 ws = twiddle2(a.post_a, a.post_b, es, a.post_shift);
-            const float2 w1 = cmulf(w0, ws);
-            const float2 s2 = cmulf(ws, ws);
-            uint64_t wr = f2p(w0.x, w1.x), wi = f2p(w0.y, w1.y);
-            const uint64_t s2r = f2p(s2.x, s2.x), s2i = f2p(s2.y, s2.y);
-            sm100::tmem_wait_ld();
-#pragma unroll
-            for (int p = 0; p < 8; ++p) {
-              uint64_t yr, yi;
-              cmul2(f2p(__uint_as_float(d[4 * p]), __uint_as_float(d[4 * p + 1])),
-                    f2p(__uint_as_float(d[4 * p + 2]), __uint_as_float(d[4 * p + 3])), wr, wi, yr,
-                    yi);
-              float r0, r1, i0, i1;
-              f2u(yr, r0, r1);
-              f2u(yi, i0, i1);
-              sts32w(xo(dst, a.kofs[s][2 * p], bb), sm100::pack_half2(r0, i0));
-              sts32w(xo(dst, a.kofs[s][2 * p + 1], bb), sm100::pack_half2(r1, i1));
-              if (p < 7) {
-                uint64_t nr, ni;
-                cmul2(wr, wi, s2r, s2i, nr, ni);
-                wr = nr;
-                wi = ni;
-              }
-            }
-          } else {
-            sm100::tmem_wait_ld();
-#pragma unroll
-            for (int p = 0; p < 8; ++p) {
-              sts32w(xo(dst, a.kofs[s][2 * p], bb),
-                     sm100::pack_half2(__uint_as_float(d[4 * p]), __uint_as_float(d[4 * p + 2])));
-              sts32w(xo(dst, a.kofs[s][2 * p + 1], bb),
-                     sm100::pack_half2(__uint_as_float(d[4 * p + 1]), __uint_as_float(d[4 * p + 3])));
-            }
-          }
-        }
-        mphase ^= 1u;
-        sm100::fence_proxy_async_smem();
-        sm100::tc_fence_before();
-        tile::named_bar(1, NCT);
-        sm100::tc_fence_after();
-        if (*abort_flag) break;
-      }
+      TL::run(a, x, tid, b, t % a.col_blocks, mphase, ient, eent);
       if (*abort_flag) break;
-      if (ctid == 0) tile::mbar_arrive(&outrdy[b]);
+      if (tid == 0) tile::mbar_arrive(&outrdy[b]);
     }
   }
   __syncthreads();

@@ -138,6 +138,10 @@ Staging make_staging(Kind kind, int L, int C, int elem, int64_t sp, int64_t sc, 
     s.gdim[2] = (uint64_t)phi;             s.box[2] = (uint32_t)phi; s.gstride_bytes[2] = (uint64_t)plo * sp * elem;
     s.gdim[3] = (uint64_t)(ncols / s.E);   s.box[3] = (uint32_t)(C / s.E); s.gstride_bytes[3] = (uint64_t)s.E * elem;
     s.gdim[4] = (uint64_t)nouter;          s.box[4] = 1;             s.gstride_bytes[4] = (uint64_t)so * elem;
+    // A pass with fewer columns than C loads and stores only its own column
+    // blocks (the outermost shared-memory dimension); the tile's other
+    // columns hold stale data that is transformed but never stored.
+    if ((int64_t)s.box[3] > (int64_t)s.gdim[3]) s.box[3] = (uint32_t)s.gdim[3];
     s.cmul[3] = C / s.E;
     s.omul[4] = 1;
     if (nouter <= 1) s.ndims = 4;

@@ -35,6 +35,14 @@ struct Staging {
   int row_bytes = 0;
   int swz = 0;                 // XOR mask applied to bits 4.. from bits 7.. (0, 1, 3, 7)
   uint32_t bytes() const { return (uint32_t)L * C * elem; }
+  // Bytes one TMA box moves (less than bytes() when the column blocks of a
+  // column staging are clamped to a pass with fewer columns than C).
+  uint32_t box_bytes() const {
+    uint32_t v = (uint32_t)elem;
+    for (int d = 0; d < ndims; ++d) v *= box[d];
+    return v;
+  }
+  bool clamped() const { return box_bytes() != bytes(); }
   uint32_t offset(uint32_t pos, uint32_t c) const;
   // TMA box: dims innermost first.  For the kernel: coordinate of dim d for
   // tile (outer, cb) is cb * cmul[d] + outer * omul[d].

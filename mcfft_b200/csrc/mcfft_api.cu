@@ -7,8 +7,8 @@
 // length-L transform (L = 16^a * R) along one axis, and picks a tile shape
 // for each pass from the instantiated kernel variants.
 //
-//   1D, n <= 8192        one row pass
-//   1D, n > 8192         four-step: n = n1 * n2; pass 1 = n1-point column
+//   1D, n <= 4096        one row pass
+//   1D, n > 4096         four-step: n = n1 * n2; pass 1 = n1-point column
 //                        transforms (stride n2) with the W_n^(k1 n2)
 //                        twiddle fused into their epilogue, into a scratch
 //                        buffer; pass 2 = n2-point row transforms written
@@ -18,7 +18,10 @@
 //
 // All tables (stage twiddles, tail twiddles, four-step twiddles, the DFT-16
 // embedding) are generated in FP64 on the GPU at plan time for both
-// directions.
+// directions.  When every pass of a plan runs on the plain 16K-point tile
+// kernel, exec is one launch of the persistent batch kernel (fft_queue.cuh)
+// over a queue of (pass, tile) items built here; otherwise one launch per
+// pass.
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
@@ -30,6 +33,7 @@
 
 #include "../../include/mcfft.h"
 #include "mcfft_internal.h"
+#include "queue.h"
 #include "tile_pass.h"
 
 namespace mcfft {
@@ -52,6 +56,27 @@ struct Pass {
   const float2* tail[2] = {nullptr, nullptr};
   const float2* plo[2] = {nullptr, nullptr};
   const float2* phi[2] = {nullptr, nullptr};
+  // Place in its transform group (one descriptor) and dependency data for
+  // the batch queue: a pass at level > 0 reads what the previous pass of its
+  // group wrote.  Producer side: tile t completes keys [t sig_mul / sig_div,
+  // ((t + 1) sig_mul - 1) / sig_div]; consumer side: tile (cb, outer) needs
+  // key `outer` complete, i.e. wait_count producer tiles; `keys` = nouter.
+  int grp = -1, level = 0;
+  int64_t sig_mul = 1, sig_div = 1;
+  int wait_count = 0;
+  int64_t keys = 0;
+};
+
+// The batch queue of a plan: every pass in one persistent launch.
+struct Queue {
+  bool on = false;
+  QItem* items = nullptr;  // device
+  int64_t nitems = 0;
+  int* counters = nullptr;  // device
+  int64_t ncounters = 0;
+  std::vector<int> wait_base, sig_base;  // per pass
+  int grid = 0;
+  QArgs* args = nullptr;  // host staging of the parameter block
 };
 
 }  // namespace
@@ -73,6 +98,8 @@ struct mcfftPlan_st {
   int* status = nullptr;
   cudaStream_t last_stream = nullptr;
   mcfftPlanInfo info{};
+  mcfft::Queue q;
+  int ngroups = 0;
 };
 
 namespace mcfft {
@@ -230,6 +257,9 @@ mcfftResult add_tile_pass(mcfftPlan p, const PassSpec& s) {
     if (!tile_layout(&tp.lay, cand->L, cand->R, cand->C, ik, ok, in_elem, out_elem, s.in_sp,
                      s.in_sc, s.in_so, s.out_sp, s.out_sc, s.out_so, s.ncols, s.nouter, &err))
       continue;
+    // the split form's tile maximum must not see the stale columns of a
+    // clamped tile
+    if (p->split && (tp.lay.in.clamped() || tp.lay.out.clamped())) continue;
     if (!tile_check_encode(tp.lay.in, p->status) || !tile_check_encode(tp.lay.out, p->status))
       continue;
     k = cand;
@@ -380,11 +410,12 @@ mcfftResult add_pass(mcfftPlan p, const PassSpec& s) {
 }
 
 constexpr int64_t kMaxSinglePass = 8192;
+constexpr int64_t kMaxTilePass = 4096;  // 1D lengths above run as four-step
 
 // Appends the passes of one transform group.  `in_buf/out_buf` and offsets
 // locate it inside the user's buffers; the first pass reads in_buf, the
 // last writes out_buf.
-mcfftResult build_group(mcfftPlan p, int ndim, const int64_t* dims, int64_t batch,
+mcfftResult build_group_passes(mcfftPlan p, int ndim, const int64_t* dims, int64_t batch,
                         int64_t in_off, int64_t out_off, int* scale_log2) {
   const bool split = p->split;
   const int in_f16 = split ? ((p->flags & MCFFT_FLAG_INPUT_F16) ? 1 : 0) : 1;
@@ -397,7 +428,7 @@ mcfftResult build_group(mcfftPlan p, int ndim, const int64_t* dims, int64_t batc
   *scale_log2 = split ? 0 : -ilog2(total);
   if (ndim == 1) {
     const int64_t n = dims[0];
-    if (n <= kMaxSinglePass) {
+    if (n <= kMaxTilePass) {
       PassSpec s{n, false, false, 1, n, 0, 1, n, 0, batch, 1, kUserIn, kUserOut, 0,
                  in_f16, split ? 0 : 1, in_off, out_off};
       return add_pass(p, s);
@@ -409,18 +440,21 @@ mcfftResult build_group(mcfftPlan p, int ndim, const int64_t* dims, int64_t batc
     const int64_t n1 = int64_t(1) << lg1, n2 = n >> lg1;
     if (n1 < 16 || n2 < 16 || n1 > kMaxSinglePass || n2 > kMaxSinglePass)
       return MCFFT_UNSUPPORTED_SIZE;
+    // Every four-step group has its own scratch region (groups of one plan
+    // may run concurrently in the batch queue).
+    const size_t ebytes = split ? 8 : 4;
+    const int64_t soff = (int64_t)(p->scratch_bytes / ebytes);
     // pass 1: columns n2, points n1 at stride n2, four-step twiddle
     PassSpec s1{n1, true, true, n2, 1, n, n2, 1, n, n2, batch, kUserIn, kScratch, n,
-                in_f16, mid_f16, in_off, 0};
+                in_f16, mid_f16, in_off, soff};
     mcfftResult r = add_pass(p, s1);
     if (r) return r;
     // pass 2: rows k1 (stride n2) of n2 points; output X[k1 + n1 k2]
     PassSpec s2{n2, false, false, 1, n2, n, n1, 1, n, n1, batch, kScratch, kUserOut, 0,
-                mid_f16, split ? 0 : 1, 0, out_off};
+                mid_f16, split ? 0 : 1, soff, out_off};
     r = add_pass(p, s2);
     if (r) return r;
-    const size_t need = (size_t)n * batch * (split ? 8 : 4);
-    p->scratch_bytes = std::max(p->scratch_bytes, need);
+    p->scratch_bytes += (size_t)n * batch * ebytes;
     return MCFFT_SUCCESS;
   }
   for (int d = 0; d < ndim; ++d)
@@ -496,15 +530,191 @@ mcfftResult plan_begin(mcfftPlan* out, mcfftPrecision prec, unsigned flags, mcff
   return MCFFT_SUCCESS;
 }
 
+// Group index, level and batch-queue dependency data of the passes
+// [first, end) of one transform group.
+void link_group(mcfftPlan p, size_t first, int ndim, const int64_t* dims, int64_t batch) {
+  const int g = p->ngroups++;
+  for (size_t i = first; i < p->passes.size(); ++i) {
+    p->passes[i].grp = g;
+    p->passes[i].level = (int)(i - first);
+  }
+  if (p->passes.size() - first < 2) return;
+  for (size_t i = first; i < p->passes.size(); ++i)
+    if (!p->passes[i].tiled) return;  // the queue only runs tile passes
+  auto C = [&](size_t i) -> int64_t { return p->passes[i].tp.k->C; };
+  auto CB = [&](size_t i) -> int64_t { return p->passes[i].tp.args.col_blocks; };
+  Pass& P0 = p->passes[first];
+  Pass& P1 = p->passes[first + 1];
+  if (ndim == 1) {  // four-step: key = transform
+    P0.sig_mul = 1;
+    P0.sig_div = CB(first);
+    P1.wait_count = (int)CB(first);
+    P1.keys = batch;
+  } else if (ndim == 2) {  // rows, then columns: key = 2D transform
+    const int64_t nx = dims[0], c = C(first);
+    P0.sig_mul = c;
+    P0.sig_div = nx;
+    P1.wait_count = (int)std::max<int64_t>(1, nx / c);
+    P1.keys = batch;
+  } else {  // z rows, y columns (key = x slab), x columns (key = 3D transform)
+    const int64_t nx = dims[0], ny = dims[1], c = C(first);
+    Pass& P2 = p->passes[first + 2];
+    P0.sig_mul = c;
+    P0.sig_div = ny;
+    P1.wait_count = (int)std::max<int64_t>(1, ny / c);
+    P1.keys = nx * batch;
+    P1.sig_mul = 1;
+    P1.sig_div = CB(first + 1) * nx;
+    P2.wait_count = (int)(CB(first + 1) * nx);
+    P2.keys = batch;
+  }
+}
+
+mcfftResult build_group(mcfftPlan p, int ndim, const int64_t* dims, int64_t batch,
+                        int64_t in_off, int64_t out_off, int* scale_log2) {
+  const size_t first = p->passes.size();
+  mcfftResult r = build_group_passes(p, ndim, dims, batch, in_off, out_off, scale_log2);
+  if (!r) link_group(p, first, ndim, dims, batch);
+  return r;
+}
+
+// Builds the batch queue (every pass of the plan in one persistent launch)
+// for plans of several transform groups (uneven batches) -- or any plan
+// with MCFFT_QUEUE=1; MCFFT_QUEUE=0 disables it -- when every pass runs on
+// the 16K-point plain tile kernel and the passes fit the kernel's parameter
+// block; otherwise the plan launches pass by pass (one transform shape is
+// faster that way: each pass kernel keeps its tables in its parameter
+// block).
+// Queue order: per transform group, the first pass's tiles in chunks of
+// four per CTA, each later pass's tile for key k once the previous pass's
+// tiles for keys up to k + W are queued (W ~ four tiles per CTA of lag), so
+// every dependency points backwards, a CTA runs several tiles of one pass
+// in a row (its tables stay in shared memory), and the intermediate is read
+// back while it is in L2.
+mcfftResult build_queue(mcfftPlan p) {
+  if (p->split) return MCFFT_SUCCESS;
+  bool want = p->ngroups > 1;
+  if (const char* e = std::getenv("MCFFT_QUEUE")) want = std::atoi(e) != 0;
+  if (!want) return MCFFT_SUCCESS;
+  const size_t np = p->passes.size();
+  if (np > (size_t)kQueueMaxPasses) return MCFFT_SUCCESS;
+  for (const auto& ps : p->passes)
+    if (!ps.tiled || ps.tp.k->split ||
+        queue_variant(ps.tp.k->L, ps.tp.k->posttw, ps.tp.k->tile_points) < 0) {
+      if (std::getenv("MCFFT_DEBUG_PLAN"))
+        fprintf(stderr, "[mcfft] no batch queue: pass L=%lld not on a queue tile variant\n",
+                (long long)(ps.tiled ? ps.tp.k->L : ps.k->L));
+      return MCFFT_SUCCESS;
+    }
+  const int maxg = queue_max_grid(p->sms);
+  if (maxg <= 0) return MCFFT_SUCCESS;
+  Queue& q = p->q;
+  q.wait_base.assign(np, -1);
+  q.sig_base.assign(np, -1);
+  int64_t nc = 0;
+  for (size_t i = 0; i < np; ++i)
+    if (p->passes[i].level > 0) {
+      q.wait_base[i] = (int)nc;
+      q.sig_base[i - 1] = (int)nc;
+      nc += p->passes[i].keys;
+    }
+  std::vector<QItem> items;
+  const int64_t G = maxg;
+  for (size_t i = 0; i < np;) {
+    size_t j = i;
+    while (j < np && p->passes[j].grp == p->passes[i].grp) ++j;
+    const int nl = (int)(j - i);
+    std::vector<int64_t> tot(nl), em(nl, 0), W(nl, 0);
+    for (int l = 0; l < nl; ++l) tot[l] = p->passes[i + l].tp.args.ntiles;
+    for (int l = 1; l < nl; ++l) {
+      const Pass& P = p->passes[i + l - 1];
+      W[l] = std::max<int64_t>(1, (4 * G * P.sig_mul + P.sig_div - 1) / P.sig_div);
+    }
+    for (bool left = true; left;) {
+      for (int64_t c = 0; c < 4 * G && em[0] < tot[0]; ++c)
+        items.push_back({(uint32_t)i, (uint32_t)em[0]++});
+      for (int l = 1; l < nl; ++l) {
+        const Pass& P = p->passes[i + l - 1];
+        const Pass& Q = p->passes[i + l];
+        while (em[l] < tot[l]) {
+          const int64_t key = em[l] / Q.tp.args.col_blocks;
+          const bool all = em[l - 1] == tot[l - 1];
+          const int64_t done = em[l - 1] * P.sig_mul / P.sig_div;
+          if (!all && done < key + 1 + W[l]) break;
+          items.push_back({(uint32_t)(i + l), (uint32_t)em[l]++});
+        }
+      }
+      left = false;
+      for (int l = 0; l < nl; ++l) left |= em[l] < tot[l];
+    }
+    i = j;
+  }
+  mcfftResult r = plan_alloc(p, &q.items, items.size() * sizeof(QItem));
+  if (!r) r = plan_alloc(p, &q.counters, (size_t)std::max<int64_t>(nc, 1) * sizeof(int));
+  if (r) return r;
+  cudaError_t e = cudaMemcpy(q.items, items.data(), items.size() * sizeof(QItem),
+                             cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) return cuda_fail(e);
+  q.nitems = (int64_t)items.size();
+  q.ncounters = nc;
+  q.grid = (int)std::min<int64_t>(G, q.nitems);
+  q.args = new (std::nothrow) QArgs();
+  if (!q.args) return MCFFT_ALLOC_FAILED;
+  q.on = true;
+  return MCFFT_SUCCESS;
+}
+
+mcfftResult exec_queue(mcfftPlan p, const void* in, void* out, int dir, cudaStream_t st) {
+  Queue& q = p->q;
+  QArgs& A = *q.args;
+  A.items = q.items;
+  A.nitems = q.nitems;
+  A.counters = q.counters;
+  A.status = p->status;
+  A.bmat = p->bsw64[dir];
+  A.npass = (int)p->passes.size();
+  auto base = [&](int b) -> char* {
+    return b == kUserIn ? (char*)const_cast<void*>(in) : b == kUserOut ? (char*)out : (char*)p->scratch;
+  };
+  for (size_t i = 0; i < p->passes.size(); ++i) {
+    const Pass& ps = p->passes[i];
+    QPass& Q = A.pass[i];
+    if (!fill_qpass(ps.tp, dir, base(ps.in_buf) + ps.in_off * 4, base(ps.out_buf) + ps.out_off * 4, &Q))
+      return MCFFT_CUDA_ERROR;
+    Q.wait_base = q.wait_base[i];
+    Q.wait_count = ps.wait_count;
+    Q.sig_base = q.sig_base[i];
+    Q.sig_mul = ps.sig_mul;
+    Q.sig_div = ps.sig_div;
+    Q.sig_kmax = q.sig_base[i] >= 0 ? p->passes[i + 1].keys - 1 : 0;
+  }
+  cudaError_t e = q.ncounters ? cudaMemsetAsync(q.counters, 0, q.ncounters * sizeof(int), st)
+                              : cudaSuccess;
+  if (e == cudaSuccess) e = launch_queue(A, q.grid, st);
+  if (e == cudaSuccess && std::getenv("MCFFT_DEBUG_SYNC")) {
+    e = cudaStreamSynchronize(st);
+    fprintf(stderr, "[mcfft] queue: %d passes, %lld items, grid %d: %s\n", A.npass,
+            (long long)q.nitems, q.grid, cudaGetErrorString(e));
+  }
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return MCFFT_CUDA_ERROR;
+  }
+  p->last_stream = st;
+  return MCFFT_SUCCESS;
+}
+
 mcfftResult plan_finish(mcfftPlan p, mcfftPlan* out) {
   mcfftResult r = MCFFT_SUCCESS;
   if (p->scratch_bytes) r = plan_alloc(p, &p->scratch, p->scratch_bytes);
+  if (!r) r = build_queue(p);
   if (!r) r = cuda_fail(cudaDeviceSynchronize());
   if (r) {
     mcfftPlanDestroy(p);
     return r;
   }
   p->info.num_passes = (int)p->passes.size();
+  p->info.launches = p->q.on ? 1 : (int)p->passes.size();
   p->info.workspace_bytes = (int64_t)p->scratch_bytes;
   *out = p;
   return MCFFT_SUCCESS;
@@ -528,13 +738,27 @@ mcfftResult mcfftPlanCreateBatch(mcfftPlan* plan, const mcfftDesc* descs, int co
   mcfftResult r = plan_begin(plan, precision, flags, &p);
   if (r) return r;
   int64_t elements = 0;
-  for (int i = 0; i < count && !r; ++i) {
+  // Consecutive descriptors of one shape whose data follow each other in
+  // both buffers form one batched group (one set of passes).
+  auto points = [](const mcfftDesc& d) {
+    int64_t t = 1;
+    for (int k = 0; k < d.ndim; ++k) t *= d.dims[k];
+    return t;
+  };
+  for (int i = 0; i < count && !r;) {
+    mcfftDesc g = descs[i];
+    int j = i + 1;
+    for (; j < count; ++j) {
+      const mcfftDesc& d = descs[j];
+      bool same = d.ndim == g.ndim;
+      for (int k = 0; k < g.ndim && same; ++k) same = d.dims[k] == g.dims[k];
+      const int64_t len = g.batch * points(g);
+      if (!same || d.in_offset != g.in_offset + len || d.out_offset != g.out_offset + len) break;
+      g.batch += d.batch;
+    }
     int sl = 0;
-    r = build_group(p, descs[i].ndim, descs[i].dims, descs[i].batch, descs[i].in_offset,
-                    descs[i].out_offset, &sl);
-    int64_t t = descs[i].batch;
-    for (int d = 0; d < descs[i].ndim; ++d) t *= descs[i].dims[d];
-    elements += t;
+    r = build_group(p, g.ndim, g.dims, g.batch, g.in_offset, g.out_offset, &sl);
+    elements += g.batch * points(g);
     if (i == 0) {
       p->info.ndim = descs[0].ndim;
       for (int d = 0; d < 3; ++d) p->info.dims[d] = d < descs[0].ndim ? descs[0].dims[d] : 1;
@@ -543,6 +767,7 @@ mcfftResult mcfftPlanCreateBatch(mcfftPlan* plan, const mcfftDesc* descs, int co
     } else if (sl != p->info.scale_log2) {
       p->info.scale_log2 = 1;  // mixed scales: 1 flags "per transform"
     }
+    i = j;
   }
   if (r) {
     mcfftPlanDestroy(p);
@@ -580,6 +805,7 @@ mcfftResult mcfftExec(mcfftPlan p, const void* in, void* out, int direction, voi
   if (direction != MCFFT_FORWARD && direction != MCFFT_INVERSE) return MCFFT_INVALID_VALUE;
   const int dir = direction == MCFFT_FORWARD ? 0 : 1;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (p->q.on) return exec_queue(p, in, out, dir, st);
   for (auto& ps : p->passes) {
     PassArgs a = ps.a;
     auto base = [&](int b) -> char* {
@@ -643,6 +869,7 @@ mcfftResult mcfftPlanGetInfo(mcfftPlan p, mcfftPlanInfo* info) {
 mcfftResult mcfftPlanDestroy(mcfftPlan p) {
   if (!p) return MCFFT_INVALID_PLAN;
   for (void* d : p->allocs) cudaFree(d);
+  delete p->q.args;
   delete p;
   return MCFFT_SUCCESS;
 }

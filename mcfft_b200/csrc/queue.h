@@ -1,0 +1,19 @@
+// queue.h -- host interface of the persistent batch kernel.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "fft_queue.cuh"
+#include "tile_pass.h"
+
+namespace mcfft {
+
+// Variant index of a pass in the batch kernel, or -1 if it has none.
+int queue_variant(int L, bool posttw, int tile_points);
+// Queue entry of a tile pass for one exec: tensor maps over in/out, tables
+// for direction `dir`; dependencies unset.  False if encoding fails.
+bool fill_qpass(const TilePass& tp, int dir, const void* in, void* out, QPass* q);
+cudaError_t launch_queue(const QArgs& a, int grid, cudaStream_t st);
+// CTAs of the batch kernel that can be resident at once (0 on error).
+int queue_max_grid(int sms);
+
+}  // namespace mcfft

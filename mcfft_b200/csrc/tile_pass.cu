@@ -121,6 +121,10 @@ bool tile_layout(layout::PassLayout* out, int L, int R, int C, layout::Kind ik, 
   return true;
 }
 
+bool tile_encode(CUtensorMap* map, const layout::Staging& s, const void* base) {
+  return encode(map, s, base);
+}
+
 bool tile_check_encode(const layout::Staging& s, const void* probe) {
   CUtensorMap m;
   return encode(&m, s, probe);
@@ -168,7 +172,7 @@ void fill_tile_args(TilePass* tp) {
     a.out_cmul[d] = l.out.cmul[d];
     a.out_omul[d] = l.out.omul[d];
   }
-  a.in_tile_bytes = l.in.bytes();
+  a.in_tile_bytes = l.in.box_bytes();
   for (size_t i = 0; i < l.lofs.size() && i < 16; ++i) a.lofs[i] = l.lofs[i];
   for (size_t i = 0; i < l.sofs.size() && i < 32; ++i) a.sofs[i] = l.sofs[i];
   for (int s = 0; s < l.NST && s < kMaxStages; ++s)

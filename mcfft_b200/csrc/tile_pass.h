@@ -43,6 +43,7 @@ bool tile_layout(layout::PassLayout* out, int L, int R, int C, layout::Kind ik, 
                  int in_elem, int out_elem, int64_t isp, int64_t isc, int64_t iso, int64_t osp,
                  int64_t osc, int64_t oso, int64_t ncols, int64_t nouter, std::string* err);
 bool tile_check_encode(const layout::Staging& s, const void* probe);
+bool tile_encode(CUtensorMap* map, const layout::Staging& s, const void* base);
 void fill_tile_args(TilePass* tp);
 cudaError_t launch_tile_pass(const TilePass& tp, const void* in, void* out, int dir,
                              cudaStream_t st);
