@@ -47,6 +47,7 @@ struct alignas(64) QPass {
   const float2* post_b;
   uint64_t post_mask;
   uint32_t post_shift;
+  float post_scale;
   int inverse;
   int32_t in_cmul[5], in_omul[5], out_cmul[5], out_omul[5];
   int32_t in_ndims, out_ndims;

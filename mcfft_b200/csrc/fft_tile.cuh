@@ -58,6 +58,7 @@ struct alignas(64) TileArgs {
   const float2* post_b;    // four-step: W_N^(e << post_shift) high table
   uint64_t post_mask;      // N - 1
   uint32_t post_shift;
+  float post_scale;        // 2 / N when N <= 2^24 (four-step twiddles by sincospif), else 0
   float out_scale;         // split form: applied after the last stage (the plain form keeps its 1/16 per stage in the DFT-16 matrix)
   int inverse;
   int split_in_f16;
@@ -349,6 +350,35 @@ __device__ __forceinline__ void small_dft_h2(__half2 (&x)[R], float sgn) {
   }
 }
 
+// Four-step twiddles of this thread's epilogue rows, w[j] = {W_N^(v g),
+// W_N^(NV g)} for row j (vector v of column g), computed before the MMA
+// wait so that their cost overlaps it.  N <= 2^24: FP32 sincospif of the
+// exact angle e (2 / N) (e / N is exact in FP32); larger N: the two-level
+// table product lo[e & (2^sh - 1)] * hi[e >> sh].
+template <int C, int NV, int NIT_E, int NST, class A>
+__device__ __forceinline__ void post_twiddles(const A& a, int64_t cb, int s,
+                                              const uint32_t (&eent)[NST][NIT_E],
+                                              float2 (&w)[NIT_E][2]) {
+  const float sgn = a.inverse ? 1.f : -1.f;
+  const uint64_t lmask = (1ull << a.post_shift) - 1;
+#pragma unroll
+  for (int j = 0; j < NIT_E; ++j) {
+    const uint32_t aux = eent[s][j] >> 16;
+    const uint64_t g = (uint64_t)(cb * C + aux % C);
+    const uint64_t e[2] = {((uint64_t)(aux / C) * g) & a.post_mask, ((uint64_t)NV * g) & a.post_mask};
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      if (a.post_scale != 0.f) {
+        float sn, cs;
+        sincospif((float)e[h] * a.post_scale, &sn, &cs);
+        w[j][h] = make_float2(cs, sgn * sn);
+      } else {
+        w[j][h] = cmulf(__ldg(a.post_a + (e[h] & lmask)), __ldg(a.post_b + (e[h] >> a.post_shift)));
+      }
+    }
+  }
+}
+
 // Per-CTA shared-memory and tensor-memory handles of the tile routines.
 struct TileCtx {
   uint32_t sS0, sS1, sA, sB, sTail, sTws;  // shared addresses
@@ -380,6 +410,7 @@ struct F16Tile {
   // source).  X[s] = A when NST - s is odd, staging otherwise; with an even
   // stage count the prologue transposes the staging buffer in place.
   static constexpr bool INPLACE_PROLOGUE = (S::NST % 2) == 0;
+  static constexpr int TMEM_COLS = S::TMEM_COLS;
 
   // This thread's prologue items and epilogue rows (the same for every tile
   // of a pass).
@@ -422,15 +453,12 @@ struct F16Tile {
     }
   }
 
+  // Prologue of the tile in staging buffer b (ends with the consumer
+  // barrier).
   template <class A>
-  static __device__ __forceinline__ void run(const A& a, const TileCtx& x, int ctid, int b,
-                                             int64_t cb, uint32_t& mphase,  // bit m: phase of mmab[m]
-                                             const uint2 (&ient)[NIT_P],
-                                             const uint32_t (&eent)[NST][NIT_E]) {
-    const int warp = ctid >> 5, lane = ctid & 31, sp = warp & 3;
-    constexpr uint32_t IDESC = sm100::idesc_f16_f32(128, 32);
+  static __device__ __forceinline__ void prologue(const A& a, const TileCtx& x, int ctid, int b,
+                                                  const uint2 (&ient)[NIT_P]) {
     const float tsgn = a.inverse ? 1.f : -1.f;
-    const uint32_t sb = b ? x.sS1 : x.sS0;
     // ---------------------------------------------------------- prologue
     // Offsets are XOR-linear relative to their buffer.
     const uint32_t bb = b ? x.bS1 : x.bS0;
@@ -470,8 +498,8 @@ struct F16Tile {
         // column items (all four sub-vectors share the row)
         const uint32_t trow = ient[j].y & 0x7FFFFFFFu;
         const bool colitem = (ient[j].y >> 31) != 0;
-#pragma unroll
-        for (int jj = 0; jj < 4; ++jj) {
+        // Sub-vector jj: radix-R butterflies, twiddles from row tw(jj), stores.
+        auto subvec = [&](int jj, auto tw_of) {
           __half2 hv[R];
 #pragma unroll
           for (int n = 0; n < R; ++n) {
@@ -479,11 +507,9 @@ struct F16Tile {
             hv[n] = *reinterpret_cast<const __half2*>(&w);
           }
           small_dft_h2<R>(hv, tsgn);
-          const uint32_t vr = colitem ? trow : trow + jj;
-          const uint32_t twa = x.sTail + vr * (R * 8);
 #pragma unroll
           for (int k2 = 0; k2 < R / 2; ++k2) {
-            const uint4 tw = tile::lds128(twa + 16 * k2);
+            const uint4 tw = tw_of(k2);
             const __half2 y0 = h2cmul(hv[2 * k2], *reinterpret_cast<const __half2*>(&tw.x),
                                       *reinterpret_cast<const __half2*>(&tw.y));
             const __half2 y1 = h2cmul(hv[2 * k2 + 1], *reinterpret_cast<const __half2*>(&tw.z),
@@ -491,6 +517,18 @@ struct F16Tile {
             sts32w(xo(st, a.sofs[jj * R + 2 * k2], x0), *reinterpret_cast<const uint32_t*>(&y0));
             sts32w(xo(st, a.sofs[jj * R + 2 * k2 + 1], x0), *reinterpret_cast<const uint32_t*>(&y1));
           }
+        };
+        if (colitem) {
+          // column items: the four sub-vectors share one twiddle row
+          uint4 twc[R / 2];
+#pragma unroll
+          for (int k2 = 0; k2 < R / 2; ++k2) twc[k2] = tile::lds128(x.sTail + trow * (R * 8) + 16 * k2);
+#pragma unroll
+          for (int jj = 0; jj < 4; ++jj) subvec(jj, [&](int k2) { return twc[k2]; });
+        } else {
+#pragma unroll
+          for (int jj = 0; jj < 4; ++jj)
+            subvec(jj, [&](int k2) { return tile::lds128(x.sTail + (trow + jj) * (R * 8) + 16 * k2); });
         }
       }
     }
@@ -499,121 +537,157 @@ struct F16Tile {
     tile::named_bar(1, NCT);
     sm100::tc_fence_after();
 
-    // ------------------------------------------------------------ stages
-#pragma unroll
-    for (int s = 0; s < S::NST; ++s) {
-      const uint32_t xs = ((S::NST - s) & 1) ? x.sA : sb;       // this stage's operand
-      const uint32_t xn = ((S::NST - s) & 1) ? bb : x.bA;       // next stage's operand (window-relative)
-      // Each M-tile's two MMAs and its commit are issued by lane 0 of the
-      // sub-partition-0 warp that drains that M-tile, so four warps issue
-      // in parallel (a single issuing thread serialises ~100 cycles per
-      // tcgen05.mma).  tcgen05.commit tracks the issuing thread's MMAs.
-      if (sp == 0 && lane == 0) {
-#pragma unroll
-        for (int j = 0; j < NIT_E; ++j) {
-          const uint32_t m = (warp >> 2) + j * (NCW / 4);
-#pragma unroll
-          for (int ks = 0; ks < 2; ++ks)
-            sm100::umma_f16(x.tmem + 32u * m, tile::sdesc_sw64(xs + m * 8192u + ks * 32u),
-                            tile::sdesc_sw64(x.sB + ks * 32u), IDESC, ks);
-          sm100::umma_commit(&x.mmab[m]);
-        }
-      }
-      const bool last = s == S::NST - 1;
-      const uint32_t row0 = stage_tw_row0<L, R>(s);
+  }
+
+  // MMAs of stage s of the tile in buffer b: accumulators in TMEM columns
+  // tm + [0, 32 NMT), completion of M-tile m on bars[m].
+  static __device__ __forceinline__ void issue(const TileCtx& x, int s, int b, int ctid, uint32_t tm,
+                                               uint64_t* bars) {
+    const int warp = ctid >> 5, lane = ctid & 31, sp = warp & 3;
+    constexpr uint32_t IDESC = sm100::idesc_f16_f32(128, 32);
+    const uint32_t sb = b ? x.sS1 : x.sS0;
+    const uint32_t xs = ((S::NST - s) & 1) ? x.sA : sb;  // this stage's operand
+    // Each M-tile's two MMAs and its commit are issued by lane 0 of the
+    // sub-partition-0 warp that drains that M-tile, so four warps issue
+    // in parallel (a single issuing thread serialises ~100 cycles per
+    // tcgen05.mma).  tcgen05.commit tracks the issuing thread's MMAs.
+    if (sp == 0 && lane == 0) {
 #pragma unroll
       for (int j = 0; j < NIT_E; ++j) {
         const uint32_t m = (warp >> 2) + j * (NCW / 4);
-        const uint32_t e = eent[s][j];
-        const uint32_t aux = e >> 16;
-        const uint32_t dst = (e & 0xFFFFu) << 2;
-        // TMEM columns per lane (the DFT-16 matrix's N order): for point
-        // pair p, d[4p..4p+3] = (re_2p, re_2p+1, im_2p, im_2p+1).  The 1/16
-        // stage scale is in the matrix.
-        float4 wg[8];
-        if (!last && !T::TW_SMEM) {
-          const float4* t4 = a.tw + (size_t)(row0 + aux) * 8;
 #pragma unroll
-          for (int p = 0; p < 8; ++p) wg[p] = __ldg(t4 + (p ^ tw_fold(aux)));
-        }
-        if (!sm100::mbar_wait_bounded(&x.mmab[m], (mphase >> m) & 1u, kWaitLimit)) *x.abort_flag = 1;
-        sm100::tc_fence_after();
-        uint32_t d[32];
-        sm100::tmem_ld32(x.tmem + ((uint32_t)(32 * sp) << 16) + 32u * m, d);
-        if (!last) {
-          const uint32_t trow = x.sTws + (row0 + aux) * 128u;
-          const uint32_t fold = tw_fold(aux);
-          sm100::tmem_wait_ld();
+        for (int ks = 0; ks < 2; ++ks)
+          sm100::umma_f16(tm + 32u * m, tile::sdesc_sw64(xs + m * 8192u + ks * 32u),
+                          tile::sdesc_sw64(x.sB + ks * 32u), IDESC, ks);
+        sm100::umma_commit(&bars[m]);
+      }
+    }
+  }
+
+  // Epilogue of stage s of the tile in buffer b: waits for bars[m] (phase
+  // bit m of `phase`, toggled here), reads TMEM columns tm + .., writes the
+  // next stage's operand or, after the last stage, the output staging
+  // (ends with the consumer barrier).
+  template <int s, class A>
+  static __device__ __forceinline__ void epilogue(const A& a, const TileCtx& x, int ctid, int b,
+                                                  int64_t cb, uint32_t tm, uint64_t* bars,
+                                                  uint32_t& phase,
+                                                  const uint32_t (&eent)[NST][NIT_E]) {
+    const int warp = ctid >> 5, sp = warp & 3;
+    const uint32_t bb = b ? x.bS1 : x.bS0;
+    const uint32_t xn = ((S::NST - s) & 1) ? bb : x.bA;  // next stage's operand (window-relative)
+    const bool last = s == S::NST - 1;
+    const uint32_t row0 = stage_tw_row0<L, R>(s);
+    float2 pt[NIT_E][2];
+    if constexpr (POSTTW && s == S::NST - 1) post_twiddles<C, S::NV>(a, cb, s, eent, pt);
 #pragma unroll
-          for (int h = 0; h < 2; ++h) {
-            float4 w[4];
+    for (int j = 0; j < NIT_E; ++j) {
+      const uint32_t m = (warp >> 2) + j * (NCW / 4);
+      const uint32_t e = eent[s][j];
+      const uint32_t aux = e >> 16;
+      const uint32_t dst = (e & 0xFFFFu) << 2;
+      // TMEM columns per lane (the DFT-16 matrix's N order): for point
+      // pair p, d[4p..4p+3] = (re_2p, re_2p+1, im_2p, im_2p+1).  The 1/16
+      // stage scale is in the matrix.
+      float4 wg[8];
+      if (!last && !T::TW_SMEM) {
+        const float4* t4 = a.tw + (size_t)(row0 + aux) * 8;
 #pragma unroll
-            for (int pp = 0; pp < 4; ++pp)
-              w[pp] = T::TW_SMEM ? lds128f(trow + (((4 * h + pp) ^ fold) << 4)) : wg[4 * h + pp];
+        for (int p = 0; p < 8; ++p) wg[p] = __ldg(t4 + (p ^ tw_fold(aux)));
+      }
+      if (!sm100::mbar_wait_bounded(&bars[m], (phase >> m) & 1u, kWaitLimit)) *x.abort_flag = 1;
+      sm100::tc_fence_after();
+      uint32_t d[32];
+      sm100::tmem_ld32(tm + ((uint32_t)(32 * sp) << 16) + 32u * m, d);
+      if (!last) {
+        const uint32_t trow = x.sTws + (row0 + aux) * 128u;
+        const uint32_t fold = tw_fold(aux);
+        sm100::tmem_wait_ld();
 #pragma unroll
-            for (int pp = 0; pp < 4; ++pp) {
-              const int p = 4 * h + pp;
-              uint64_t yr, yi;
-              cmul2(f2p(__uint_as_float(d[4 * p]), __uint_as_float(d[4 * p + 1])),
-                    f2p(__uint_as_float(d[4 * p + 2]), __uint_as_float(d[4 * p + 3])),
-                    f2p(w[pp].x, w[pp].y), f2p(w[pp].z, w[pp].w), yr, yi);
-              float r0, r1, i0, i1;
-              f2u(yr, r0, r1);
-              f2u(yi, i0, i1);
-              sts32w(xo(dst, a.kofs[s][2 * p], xn), sm100::pack_half2(r0, i0));
-              sts32w(xo(dst, a.kofs[s][2 * p + 1], xn), sm100::pack_half2(r1, i1));
-            }
-          }
-        } else if (POSTTW) {
-          // Four-step twiddle W_N^((v + NV k) g): pairs (w_2p, w_2p+1)
-          // from w_0 = W_N^(v g) and ws = W_N^(NV g), advanced by ws^2
-          // (FP32 recurrence, 7 steps, far below the FP16 output rounding).
-          const uint32_t v = aux / C, c = aux % C;
-          const uint64_t g = (uint64_t)(cb * C + c);
-          const uint64_t e0 = ((uint64_t)v * g) & a.post_mask;
-          const uint64_t es = ((uint64_t)S::NV * g) & a.post_mask;
-          const float2 w0 = twiddle2(a.post_a, a.post_b, e0, a.post_shift);
-          const float2 ws = twiddle2(a.post_a, a.post_b, es, a.post_shift);
-          const float2 w1 = cmulf(w0, ws);
-          const float2 s2 = cmulf(ws, ws);
-          uint64_t wr = f2p(w0.x, w1.x), wi = f2p(w0.y, w1.y);
-          const uint64_t s2r = f2p(s2.x, s2.x), s2i = f2p(s2.y, s2.y);
-          sm100::tmem_wait_ld();
+        for (int h = 0; h < 2; ++h) {
+          float4 w[4];
 #pragma unroll
-          for (int p = 0; p < 8; ++p) {
+          for (int pp = 0; pp < 4; ++pp)
+            w[pp] = T::TW_SMEM ? lds128f(trow + (((4 * h + pp) ^ fold) << 4)) : wg[4 * h + pp];
+#pragma unroll
+          for (int pp = 0; pp < 4; ++pp) {
+            const int p = 4 * h + pp;
             uint64_t yr, yi;
             cmul2(f2p(__uint_as_float(d[4 * p]), __uint_as_float(d[4 * p + 1])),
-                  f2p(__uint_as_float(d[4 * p + 2]), __uint_as_float(d[4 * p + 3])), wr, wi, yr,
-                  yi);
+                  f2p(__uint_as_float(d[4 * p + 2]), __uint_as_float(d[4 * p + 3])),
+                  f2p(w[pp].x, w[pp].y), f2p(w[pp].z, w[pp].w), yr, yi);
             float r0, r1, i0, i1;
             f2u(yr, r0, r1);
             f2u(yi, i0, i1);
-            sts32w(xo(dst, a.kofs[s][2 * p], bb), sm100::pack_half2(r0, i0));
-            sts32w(xo(dst, a.kofs[s][2 * p + 1], bb), sm100::pack_half2(r1, i1));
-            if (p < 7) {
-              uint64_t nr, ni;
-              cmul2(wr, wi, s2r, s2i, nr, ni);
-              wr = nr;
-              wi = ni;
-            }
-          }
-        } else {
-          sm100::tmem_wait_ld();
-#pragma unroll
-          for (int p = 0; p < 8; ++p) {
-            sts32w(xo(dst, a.kofs[s][2 * p], bb),
-                   sm100::pack_half2(__uint_as_float(d[4 * p]), __uint_as_float(d[4 * p + 2])));
-            sts32w(xo(dst, a.kofs[s][2 * p + 1], bb),
-                   sm100::pack_half2(__uint_as_float(d[4 * p + 1]), __uint_as_float(d[4 * p + 3])));
+            sts32w(xo(dst, a.kofs[s][2 * p], xn), sm100::pack_half2(r0, i0));
+            sts32w(xo(dst, a.kofs[s][2 * p + 1], xn), sm100::pack_half2(r1, i1));
           }
         }
+      } else if (POSTTW) {
+        // Four-step twiddle W_N^((v + NV k) g): pairs (w_2p, w_2p+1)
+        // from w_0 = W_N^(v g) and ws = W_N^(NV g), advanced by ws^2
+        // (FP32 recurrence, 7 steps, far below the FP16 output rounding).
+        const float2 w0 = pt[j][0];
+        const float2 ws = pt[j][1];
+        const float2 w1 = cmulf(w0, ws);
+        const float2 s2 = cmulf(ws, ws);
+        uint64_t wr = f2p(w0.x, w1.x), wi = f2p(w0.y, w1.y);
+        const uint64_t s2r = f2p(s2.x, s2.x), s2i = f2p(s2.y, s2.y);
+        sm100::tmem_wait_ld();
+#pragma unroll
+        for (int p = 0; p < 8; ++p) {
+          uint64_t yr, yi;
+          cmul2(f2p(__uint_as_float(d[4 * p]), __uint_as_float(d[4 * p + 1])),
+                f2p(__uint_as_float(d[4 * p + 2]), __uint_as_float(d[4 * p + 3])), wr, wi, yr,
+                yi);
+          float r0, r1, i0, i1;
+          f2u(yr, r0, r1);
+          f2u(yi, i0, i1);
+          sts32w(xo(dst, a.kofs[s][2 * p], bb), sm100::pack_half2(r0, i0));
+          sts32w(xo(dst, a.kofs[s][2 * p + 1], bb), sm100::pack_half2(r1, i1));
+          if (p < 7) {
+            uint64_t nr, ni;
+            cmul2(wr, wi, s2r, s2i, nr, ni);
+            wr = nr;
+            wi = ni;
+          }
+        }
+      } else {
+        sm100::tmem_wait_ld();
+#pragma unroll
+        for (int p = 0; p < 8; ++p) {
+          sts32w(xo(dst, a.kofs[s][2 * p], bb),
+                 sm100::pack_half2(__uint_as_float(d[4 * p]), __uint_as_float(d[4 * p + 2])));
+          sts32w(xo(dst, a.kofs[s][2 * p + 1], bb),
+                 sm100::pack_half2(__uint_as_float(d[4 * p + 1]), __uint_as_float(d[4 * p + 3])));
+        }
       }
-      mphase ^= (1u << NMT) - 1u;
-      sm100::fence_proxy_async_smem();
-      sm100::tc_fence_before();
-      tile::named_bar(1, NCT);
-      sm100::tc_fence_after();
-      if (*x.abort_flag) break;
+    }
+    phase ^= (1u << NMT) - 1u;
+    sm100::fence_proxy_async_smem();
+    sm100::tc_fence_before();
+    tile::named_bar(1, NCT);
+    sm100::tc_fence_after();
+  }
+
+  // The whole tile, stage after stage (mphase: phase bits of x.mmab).
+  template <class A>
+  static __device__ __forceinline__ void run(const A& a, const TileCtx& x, int ctid, int b,
+                                             int64_t cb, uint32_t& mphase,
+                                             const uint2 (&ient)[NIT_P],
+                                             const uint32_t (&eent)[NST][NIT_E]) {
+    prologue(a, x, ctid, b, ient);
+    issue(x, 0, b, ctid, x.tmem, x.mmab);
+    epilogue<0>(a, x, ctid, b, cb, x.tmem, x.mmab, mphase, eent);
+    if constexpr (NST > 1) {
+      if (*x.abort_flag) return;
+      issue(x, 1, b, ctid, x.tmem, x.mmab);
+      epilogue<1 < NST ? 1 : 0>(a, x, ctid, b, cb, x.tmem, x.mmab, mphase, eent);
+    }
+    if constexpr (NST > 2) {
+      if (*x.abort_flag) return;
+      issue(x, 2, b, ctid, x.tmem, x.mmab);
+      epilogue<2 < NST ? 2 : 0>(a, x, ctid, b, cb, x.tmem, x.mmab, mphase, eent);
     }
   }
 };
@@ -665,7 +739,7 @@ __global__ void __maxnreg__(NCW <= 8 ? 80 : 96) fft_tile_f16(const __grid_consta
       sm100::fence_mbar_init();
     }
     __syncwarp();
-    sm100::tmem_alloc(tmem_slot, S::TMEM_COLS);
+    sm100::tmem_alloc(tmem_slot, TL::TMEM_COLS);
     sm100::tmem_relinquish();
   } else {
     for (int i = tid; i < 128; i += NCT)
@@ -744,7 +818,7 @@ __global__ void __maxnreg__(NCW <= 8 ? 80 : 96) fft_tile_f16(const __grid_consta
   }
   __syncthreads();
   if (tid == 0 && *abort_flag && a.status) atomicExch(a.status, kStatusTimeout);
-  if (producer) sm100::tmem_dealloc(tmem_base, S::TMEM_COLS);
+  if (producer) sm100::tmem_dealloc(tmem_base, TL::TMEM_COLS);
 }
 
 }  // namespace mcfft

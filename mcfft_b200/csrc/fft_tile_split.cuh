@@ -363,6 +363,8 @@ __global__ void __maxnreg__(96) fft_tile_split(const __grid_constant__ TileArgs 
         }
         const bool last = s == S::NST - 1;
         const uint32_t row0 = stage_tw_row0<L, R>(s);
+        float2 pt[NIT_E][2];
+        if (POSTTW && last) post_twiddles<C, S::NV>(a, cb, s, eent, pt);
 #pragma unroll
         for (int j = 0; j < NIT_E; ++j) {
           const uint32_t m = (warp >> 2) + j * (NCW / 4);
@@ -408,12 +410,8 @@ __global__ void __maxnreg__(96) fft_tile_split(const __grid_constant__ TileArgs 
             // Four-step twiddle W_N^((v + NV k) g) times L / (16 2^sexp):
             // pairs (w_2p, w_2p+1) advanced by ws^2 (FP32 recurrence, 7
             // steps, ~1e-7 relative).
-            const uint32_t v = aux / C, c = aux % C;
-            const uint64_t g = (uint64_t)(cb * C + c);
-            const uint64_t e0 = ((uint64_t)v * g) & a.post_mask;
-            const uint64_t es = ((uint64_t)S::NV * g) & a.post_mask;
-            float2 w0 = twiddle2(a.post_a, a.post_b, e0, a.post_shift);
-            const float2 ws = twiddle2(a.post_a, a.post_b, es, a.post_shift);
+            float2 w0 = pt[j][0];
+            const float2 ws = pt[j][1];
             w0.x *= fm;
             w0.y *= fm;
             const float2 w1 = cmulf(w0, ws);

@@ -310,6 +310,7 @@ mcfftResult add_tile_pass(mcfftPlan p, const PassSpec& s) {
     }
     a.post_mask = (uint64_t)s.postN - 1;
     a.post_shift = (uint32_t)sh;
+    a.post_scale = s.postN <= (int64_t(1) << 24) ? (float)(2.0 / (double)s.postN) : 0.f;
   }
   for (int dir = 0; dir < 2; ++dir) {
     tp.bmat[dir] = p->bsw64[dir];

@@ -33,6 +33,7 @@ bool fill_qpass(const TilePass& tp, int dir, const void* in, void* out, QPass* q
   q->post_b = tp.post_b[dir];
   q->post_mask = a.post_mask;
   q->post_shift = a.post_shift;
+  q->post_scale = a.post_scale;
   q->inverse = dir;
   std::memcpy(q->in_cmul, a.in_cmul, sizeof(q->in_cmul));
   std::memcpy(q->in_omul, a.in_omul, sizeof(q->in_omul));

@@ -25,7 +25,8 @@ TileKernel make_f16() {
   using T = TileF16<L, R, C, PT, NCW>;
   using S = TileShape<L, R, C, NCW>;
   return TileKernel{reinterpret_cast<const void*>(&fft_tile_f16<L, R, C, PT, NCW>),
-                    L, R, C, PT, false, S::NT, T::SMEM_BYTES, S::TMEM_COLS, TP, true};
+                    L, R, C, PT, false, S::NT, T::SMEM_BYTES, F16Tile<L, R, C, PT, NCW>::TMEM_COLS,
+                    TP, true};
 }
 
 #define MCFFT_TILE_VARIANTS(PT, TP, NCW)                                                  \
