@@ -109,7 +109,10 @@ MCFFT_API mcfftResult mcfftPlanCreateBatch(mcfftPlan* plan, const mcfftDesc* des
 
 /* Stream-ordered; `in` and `out` are device pointers (may be equal for
  * single-pass plans).  direction: MCFFT_FORWARD or MCFFT_INVERSE.  One plan
- * must not run concurrently on two streams (its workspace is shared). */
+ * must not run concurrently on two streams (its workspace is shared).
+ * The second exec on the same (in, out, direction) captures the plan's
+ * launches into a CUDA graph that later execs replay (up to four such
+ * graphs per plan; MCFFT_GRAPH=0 in the environment disables this). */
 MCFFT_API mcfftResult mcfftExec(mcfftPlan plan, const void* in, void* out, int direction,
                       void* stream);
 

@@ -312,23 +312,39 @@ __global__ void __maxnreg__(96) fft_tile_split(const __grid_constant__ TileArgs 
         } else {
           const uint32_t trow = ient[j].y & 0x7FFFFFFFu;
           const bool colitem = (ient[j].y >> 31) != 0;
-#pragma unroll
-          for (int jj = 0; jj < SUBV; ++jj) {
+          // Sub-vector jj of the unit: radix-R butterflies, twiddle times
+          // the tile scale, split, stores.
+          auto subvec = [&](int jj, auto tw_of) {
             const int sv = SUBV * h + jj;
             float2 x[R];
 #pragma unroll
             for (int n = 0; n < R; ++n) x[n] = load_point<IN16>(q[j][n], jj);
             small_dft<R>(x, tsgn);
-            const uint32_t vr = colitem ? trow : trow + sv;
 #pragma unroll
             for (int k = 0; k < R; ++k) {
-              const float2 w = lds64f(sTail + (vr * R + k) * 8);
-              const float2 y = cmulf(x[k], w);
               uint32_t hi, lo;
-              split2(make_float2(y.x * sc, y.y * sc), hi, lo);
+              split2(cmulf(x[k], tw_of(k)), hi, lo);
               sts32w(xo(st, a.sofs[sv * R + k], x0), hi);
               sts32w(xo(st, a.sofs[sv * R + k], x0l), lo);
             }
+          };
+          if (colitem) {
+            // column items: the sub-vectors share one twiddle row
+            float2 wc[R];
+#pragma unroll
+            for (int k = 0; k < R; ++k) {
+              const float2 w = lds64f(sTail + (trow * R + k) * 8);
+              wc[k] = make_float2(w.x * sc, w.y * sc);
+            }
+#pragma unroll
+            for (int jj = 0; jj < SUBV; ++jj) subvec(jj, [&](int k) { return wc[k]; });
+          } else {
+#pragma unroll
+            for (int jj = 0; jj < SUBV; ++jj)
+              subvec(jj, [&](int k) {
+                const float2 w = lds64f(sTail + ((trow + SUBV * h + jj) * R + k) * 8);
+                return make_float2(w.x * sc, w.y * sc);
+              });
           }
         }
       }

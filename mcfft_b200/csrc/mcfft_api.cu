@@ -27,6 +27,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <string>
 #include <vector>
@@ -100,6 +101,21 @@ struct mcfftPlan_st {
   mcfftPlanInfo info{};
   mcfft::Queue q;
   int ngroups = 0;
+  // Executable graphs of recent execs, keyed by (in, out, direction): an
+  // exec repeated on the same buffers replays its captured launches.
+  struct GraphEntry {
+    const void* in = nullptr;
+    void* out = nullptr;
+    int dir = -1;
+    int uses = 0;  // execs seen with this key (captured on the second)
+    cudaGraphExec_t exec = nullptr;
+    uint64_t stamp = 0;
+  };
+  GraphEntry graphs[4];
+  uint64_t graph_clock = 0;
+  bool graphs_on = true;
+  cudaStream_t capture_stream = nullptr;
+  std::mutex graph_mu;
 };
 
 namespace mcfft {
@@ -502,6 +518,8 @@ mcfftResult plan_begin(mcfftPlan* out, mcfftPrecision prec, unsigned flags, mcff
   cudaGetDevice(&p->device);
   cudaDeviceGetAttribute(&p->sms, cudaDevAttrMultiProcessorCount, p->device);
   p->split = prec == MCFFT_PREC_SPLIT;
+  if (const char* e = std::getenv("MCFFT_GRAPH")) p->graphs_on = std::atoi(e) != 0;
+  if (std::getenv("MCFFT_DEBUG_SYNC")) p->graphs_on = false;
   p->flags = flags;
   p->info.precision = (int)prec;
   mcfftResult r = plan_alloc(p, &p->status, sizeof(int));
@@ -721,6 +739,105 @@ mcfftResult plan_finish(mcfftPlan p, mcfftPlan* out) {
   return MCFFT_SUCCESS;
 }
 
+mcfftResult exec_launches(mcfftPlan p, const void* in, void* out, int dir, cudaStream_t st);
+
+// Replays the launches of an exec from a CUDA graph captured on the second
+// exec with the same buffers and direction (the first runs them directly,
+// which also completes any one-time kernel configuration).  Returns
+// MCFFT_UNSUPPORTED_SIZE when the exec should run directly instead.
+mcfftResult exec_graph(mcfftPlan p, const void* in, void* out, int dir, cudaStream_t st) {
+  std::lock_guard<std::mutex> lk(p->graph_mu);
+  if (!p->graphs_on) return MCFFT_UNSUPPORTED_SIZE;
+  mcfftPlan_st::GraphEntry* e = nullptr;
+  for (auto& g : p->graphs)
+    if (g.in == in && g.out == out && g.dir == dir) e = &g;
+  if (!e) {
+    e = &p->graphs[0];
+    for (auto& g : p->graphs)
+      if (g.stamp < e->stamp) e = &g;
+    if (e->exec) cudaGraphExecDestroy(e->exec);
+    *e = mcfftPlan_st::GraphEntry();
+    e->in = in;
+    e->out = out;
+    e->dir = dir;
+  }
+  e->stamp = ++p->graph_clock;
+  if (!e->exec && e->uses++ == 0) return MCFFT_UNSUPPORTED_SIZE;
+  if (!e->exec) {
+    if (!p->capture_stream &&
+        cudaStreamCreateWithFlags(&p->capture_stream, cudaStreamNonBlocking) != cudaSuccess) {
+      cudaGetLastError();
+      p->graphs_on = false;
+      return MCFFT_UNSUPPORTED_SIZE;
+    }
+    cudaGraph_t g = nullptr;
+    mcfftResult r = MCFFT_CUDA_ERROR;
+    if (cudaStreamBeginCapture(p->capture_stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+      r = exec_launches(p, in, out, dir, p->capture_stream);
+      if (cudaStreamEndCapture(p->capture_stream, &g) != cudaSuccess) r = MCFFT_CUDA_ERROR;
+    }
+    if (r == MCFFT_SUCCESS && g && cudaGraphInstantiate(&e->exec, g, 0) != cudaSuccess) {
+      e->exec = nullptr;
+      r = MCFFT_CUDA_ERROR;
+    }
+    if (g) cudaGraphDestroy(g);
+    if (r != MCFFT_SUCCESS) {
+      // not capturable here: run this plan's execs directly from now on
+      cudaGetLastError();
+      p->graphs_on = false;
+      return MCFFT_UNSUPPORTED_SIZE;
+    }
+  }
+  if (cudaGraphLaunch(e->exec, st) != cudaSuccess) {
+    cudaGetLastError();
+    return MCFFT_CUDA_ERROR;
+  }
+  p->last_stream = st;
+  return MCFFT_SUCCESS;
+}
+
+mcfftResult exec_launches(mcfftPlan p, const void* in, void* out, int dir, cudaStream_t st) {
+  if (p->q.on) return exec_queue(p, in, out, dir, st);
+  for (auto& ps : p->passes) {
+    PassArgs a = ps.a;
+    auto base = [&](int b) -> char* {
+      return b == kUserIn ? (char*)const_cast<void*>(in) : b == kUserOut ? (char*)out : (char*)p->scratch;
+    };
+    const int ib = p->split ? (ps.in_f16 ? 4 : 8) : 4;
+    const int ob = p->split ? (ps.out_f16 ? 4 : 8) : 4;
+    a.in = base(ps.in_buf) + ps.in_off * ib;
+    a.out = base(ps.out_buf) + ps.out_off * ob;
+    if (ps.tiled) {
+      cudaError_t e = launch_tile_pass(ps.tp, a.in, a.out, dir, st);
+      if (e == cudaSuccess && std::getenv("MCFFT_DEBUG_SYNC")) {
+        e = cudaStreamSynchronize(st);
+        fprintf(stderr, "[mcfft] tile pass L=%d R=%d C=%d grid=%d tiles=%lld: %s\n", ps.tp.k->L,
+                ps.tp.k->R, ps.tp.k->C, ps.tp.grid, (long long)ps.tp.args.ntiles,
+                cudaGetErrorString(e));
+      }
+      if (e != cudaSuccess) {
+        cudaGetLastError();
+        return MCFFT_CUDA_ERROR;
+      }
+      continue;
+    }
+    a.tw = ps.tw[dir];
+    a.tail_tw = ps.tail[dir];
+    a.post_lo = ps.plo[dir];
+    a.post_hi = ps.phi[dir];
+    a.bmat = p->bmat[dir];
+    a.bmat_lo = p->bmat_lo[dir];
+    a.inverse = dir;
+    cudaError_t e = launch_pass(*ps.k, a, ps.grid, st);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      return MCFFT_CUDA_ERROR;
+    }
+  }
+  p->last_stream = st;
+  return MCFFT_SUCCESS;
+}
+
 }  // namespace
 }  // namespace mcfft
 
@@ -806,45 +923,9 @@ mcfftResult mcfftExec(mcfftPlan p, const void* in, void* out, int direction, voi
   if (direction != MCFFT_FORWARD && direction != MCFFT_INVERSE) return MCFFT_INVALID_VALUE;
   const int dir = direction == MCFFT_FORWARD ? 0 : 1;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  if (p->q.on) return exec_queue(p, in, out, dir, st);
-  for (auto& ps : p->passes) {
-    PassArgs a = ps.a;
-    auto base = [&](int b) -> char* {
-      return b == kUserIn ? (char*)const_cast<void*>(in) : b == kUserOut ? (char*)out : (char*)p->scratch;
-    };
-    const int ib = p->split ? (ps.in_f16 ? 4 : 8) : 4;
-    const int ob = p->split ? (ps.out_f16 ? 4 : 8) : 4;
-    a.in = base(ps.in_buf) + ps.in_off * ib;
-    a.out = base(ps.out_buf) + ps.out_off * ob;
-    if (ps.tiled) {
-      cudaError_t e = launch_tile_pass(ps.tp, a.in, a.out, dir, st);
-      if (e == cudaSuccess && std::getenv("MCFFT_DEBUG_SYNC")) {
-        e = cudaStreamSynchronize(st);
-        fprintf(stderr, "[mcfft] tile pass L=%d R=%d C=%d grid=%d tiles=%lld: %s\n", ps.tp.k->L,
-                ps.tp.k->R, ps.tp.k->C, ps.tp.grid, (long long)ps.tp.args.ntiles,
-                cudaGetErrorString(e));
-      }
-      if (e != cudaSuccess) {
-        cudaGetLastError();
-        return MCFFT_CUDA_ERROR;
-      }
-      continue;
-    }
-    a.tw = ps.tw[dir];
-    a.tail_tw = ps.tail[dir];
-    a.post_lo = ps.plo[dir];
-    a.post_hi = ps.phi[dir];
-    a.bmat = p->bmat[dir];
-    a.bmat_lo = p->bmat_lo[dir];
-    a.inverse = dir;
-    cudaError_t e = launch_pass(*ps.k, a, ps.grid, st);
-    if (e != cudaSuccess) {
-      cudaGetLastError();
-      return MCFFT_CUDA_ERROR;
-    }
-  }
-  p->last_stream = st;
-  return MCFFT_SUCCESS;
+  const mcfftResult r = exec_graph(p, in, out, dir, st);
+  if (r != MCFFT_UNSUPPORTED_SIZE) return r;
+  return exec_launches(p, in, out, dir, st);
 }
 
 mcfftResult mcfftPlanCheckStatus(mcfftPlan p) {
@@ -869,6 +950,9 @@ mcfftResult mcfftPlanGetInfo(mcfftPlan p, mcfftPlanInfo* info) {
 
 mcfftResult mcfftPlanDestroy(mcfftPlan p) {
   if (!p) return MCFFT_INVALID_PLAN;
+  for (auto& g : p->graphs)
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+  if (p->capture_stream) cudaStreamDestroy(p->capture_stream);
   for (void* d : p->allocs) cudaFree(d);
   delete p->q.args;
   delete p;
