@@ -1,13 +1,13 @@
 // fft_queue.cuh -- persistent batch kernel: one launch runs every pass of a
 // plan (many transforms of uneven lengths and dimensionality) from a device
-// work queue of (pass, tile) items, plain FP16 form.
+// work queue of (pass, tile) items; one instantiation per precision form.
 //
 // Each CTA takes items blockIdx.x, blockIdx.x + gridDim.x, ... of the queue
 // in order.  Per item the producer warp issues the TMA load of the tile's
 // input and, once the consumers are done, the TMA store of its output; the
-// consumer warps run the same per-tile routine as the per-pass kernel
-// (F16Tile::run), instantiated for every pass variant (L, four-step
-// twiddle) and selected per item.  Layout tables and tensor maps of all
+// consumer warps run the same per-tile routine as the per-pass kernels
+// (F16Tile::run, SplitTile::run), instantiated for every pass variant (L,
+// four-step twiddle, tile size or input type) and selected per item.  Layout tables and tensor maps of all
 // passes live in the kernel's parameter block (constant bank).
 //
 // Dependencies between passes of one transform (the second pass of a
@@ -26,6 +26,7 @@
 // reader = acquire load, proxy fence, bulk tensor load.
 #pragma once
 #include "fft_tile.cuh"
+#include "fft_tile_split.cuh"
 
 namespace mcfft {
 
@@ -71,23 +72,26 @@ struct alignas(64) QArgs {
   int64_t nitems;
   int* counters;
   int* status;
-  const uint4* bmat;  // DFT-16 embedding (scaled by 1/16), 64B-swizzled K-major, 2 KB
+  const uint4* bmat;     // DFT-16 embedding, 64B-swizzled K-major, 2 KB (plain: scaled by 1/16)
+  const uint4* bmat_lo;  // split form: its low part
   int npass;
   QPass pass[kQueueMaxPasses];
 };
 static_assert(sizeof(QArgs) <= 32764, "kernel parameter block");
 
-// Queue-kernel shared memory: the 16K-point tile buffers, then the largest
-// radix-R and stage-row tables any variant uses.
+// Queue-kernel shared memory: three 64 KB tile buffers (16K FP16 or 8K
+// FP32 points), the DFT-16 matrices, then the largest radix-R and stage-row
+// tables any variant keeps in shared memory.
 struct QueueSmem {
-  static constexpr int STAGE_BYTES = 16384 * 4;
+  static constexpr int STAGE_BYTES = 65536;
   static constexpr int OFF_S0 = 0;
   static constexpr int OFF_S1 = STAGE_BYTES;
   static constexpr int OFF_A = 2 * STAGE_BYTES;
-  static constexpr int OFF_B = 3 * STAGE_BYTES;
-  static constexpr int OFF_TAIL = OFF_B + 2048;
+  static constexpr int OFF_B = 3 * STAGE_BYTES;        // high, then low (split) matrix
+  static constexpr int OFF_TAIL = OFF_B + 4096;
   static constexpr int OFF_TWS = OFF_TAIL + 2048 * 8;  // radix-R table of L <= 2048
-  static constexpr int OFF_BAR = OFF_TWS + 128 * 128;  // up to 128 stage rows
+  static constexpr int TWS_BYTES = 32 * 128;           // up to 32 stage rows
+  static constexpr int OFF_BAR = OFF_TWS + TWS_BYTES;
   static constexpr int SMEM_BYTES = OFF_BAR + 256;     // the window base must be 1 KB aligned
   static_assert(SMEM_BYTES <= 232448, "shared memory budget");
 };
@@ -95,12 +99,13 @@ struct QueueSmem {
 namespace queue {
 
 // Variant index of a pass: L = 32 .. 4096, with and without the four-step
-// twiddle, 16K- or 8K-point tiles (4096 only 16K);
-// variant = 16 * (8K tile) + 2 * index(L) + posttw.
-__host__ __device__ constexpr int variant_of(int L, bool posttw, int tile_points) {
+// twiddle; plain form: 16K- or 8K-point tiles (4096 only 16K), variant =
+// 16 * (8K tile) + 2 * index(L) + posttw; split form (8K tiles, L <= 2048):
+// variant = 16 * (FP16 input) + 2 * index(L) + posttw.
+__host__ __device__ constexpr int variant_of(int L, bool posttw, bool alt) {
   int i = 0;
   for (int l = 32; l < L; l <<= 1) ++i;
-  return 16 * (tile_points == 8192 ? 1 : 0) + 2 * i + (posttw ? 1 : 0);
+  return 16 * (alt ? 1 : 0) + 2 * i + (posttw ? 1 : 0);
 }
 
 }  // namespace queue
@@ -137,23 +142,20 @@ struct Variant {
   static constexpr int LI = (V >> 1) & 7;  // L = 32 << LI
   static constexpr int L = 32 << LI;
   static constexpr int R = 1 << ((5 + LI) % 4);
-  static constexpr int TP = V >= 16 ? 8192 : 16384;
-  static constexpr int C = TP / L;
   static constexpr bool PT = (V & 1) != 0;
+  static constexpr bool ALT = V >= 16;     // plain: 8K tiles; split: FP16 input
 };
 
 // Runs this CTA's consecutive items k, k+1, ... that belong to pass `pi`
-// (whose variant is V); returns the local index of the first item of
+// with tile routine TL; returns the local index of the first item of
 // another pass.  The pass's tables go to shared memory and its layout
 // entries to registers once per run.
-template <int V>
-__device__ __forceinline__ int64_t run_variant(const QArgs& a, uint32_t pi, const TileCtx& x,
-                                               uint8_t* smem, uint64_t* full, uint64_t* outrdy,
-                                               int ctid, int64_t k, int64_t nlocal,
-                                               uint32_t& mphase) {
-  using VV = Variant<V>;
-  using TL = F16Tile<VV::L, VV::R, VV::C, VV::PT, 16>;
-  static_assert(VV::C >= 4, "columns per tile");
+template <class TL, bool SPLIT, class X>
+__device__ __forceinline__ int64_t run_items(const QArgs& a, uint32_t pi, const X& x,
+                                             uint8_t* smem, uint64_t* full, uint64_t* outrdy,
+                                             int ctid, int64_t k, int64_t nlocal,
+                                             uint32_t& mphase) {
+  static_assert(!TL::T::TW_SMEM || TL::T::TW_ROWS * 128 <= QueueSmem::TWS_BYTES, "stage rows");
   const QPass& P = a.pass[pi];
   const int64_t G = gridDim.x;
   // every consumer is past the previous tile's last barrier, so nobody
@@ -163,27 +165,60 @@ __device__ __forceinline__ int64_t run_variant(const QArgs& a, uint32_t pi, cons
   uint2 ient[TL::NIT_P];
   uint32_t eent[TL::NST][TL::NIT_E];
   TL::entries(P, ctid, ient, eent);
+  volatile int* abort_flag;
+  if constexpr (SPLIT) abort_flag = x.t.abort_flag;
+  else abort_flag = x.abort_flag;
   for (;;) {
     const int b = (int)(k & 1);
     const int64_t t = a.items[blockIdx.x + k * G].tile;
-    TL::run(P, x, ctid, b, t % P.col_blocks, mphase, ient, eent);
-    if (*x.abort_flag) return nlocal;
+    if constexpr (SPLIT) {
+      TL::run(P, x, ctid, b, t % P.col_blocks, k, mphase, ient, eent);
+    } else {
+      TL::run(P, x, ctid, b, t % P.col_blocks, mphase, ient, eent);
+    }
+    if (*abort_flag) return nlocal;
     if (ctid == 0) tile::mbar_arrive(&outrdy[b]);
     if (++k >= nlocal || a.items[blockIdx.x + k * G].pass != pi) return k;
     if (!sm100::mbar_wait_bounded(&full[k & 1], (uint32_t)(k >> 1) & 1u, kWaitLimit)) {
-      *x.abort_flag = 1;
+      *abort_flag = 1;
       return nlocal;
     }
-    if (*x.abort_flag) return nlocal;
+    if (*abort_flag) return nlocal;
   }
+}
+
+template <int V>
+__device__ __forceinline__ int64_t run_variant(const QArgs& a, uint32_t pi, const TileCtx& x,
+                                               uint8_t* smem, uint64_t* full, uint64_t* outrdy,
+                                               int ctid, int64_t k, int64_t nlocal,
+                                               uint32_t& mphase) {
+  using VV = Variant<V>;
+  constexpr int C = (VV::ALT ? 8192 : 16384) / VV::L;
+  static_assert(C >= 4, "columns per tile");
+  using TL = F16Tile<VV::L, VV::R, C, VV::PT, 16>;
+  return run_items<TL, false>(a, pi, x, smem, full, outrdy, ctid, k, nlocal, mphase);
+}
+
+template <int V>
+__device__ __forceinline__ int64_t run_variant_split(const QArgs& a, uint32_t pi,
+                                                     const SplitCtx& x, uint8_t* smem,
+                                                     uint64_t* full, uint64_t* outrdy, int ctid,
+                                                     int64_t k, int64_t nlocal,
+                                                     uint32_t& mphase) {
+  using VV = Variant<V>;
+  static_assert(VV::L <= 2048, "split tiles hold at least four columns");
+  using TL = SplitTile<VV::L, VV::R, 8192 / VV::L, VV::PT, 16, VV::ALT>;
+  return run_items<TL, true>(a, pi, x, smem, full, outrdy, ctid, k, nlocal, mphase);
 }
 
 }  // namespace queue
 
 // 16 consumer warps + 1 producer warp; 96 registers (17 warps are granted
-// registers as 20).
-__global__ void __maxnreg__(96) fft_queue_f16(const __grid_constant__ QArgs a) {
-  constexpr int NCW = 16, NCT = NCW * 32, NMT = 8, TMEM_COLS = 256;
+// registers as 20).  SPLIT selects the precision form.
+template <bool SPLIT>
+__global__ void __maxnreg__(96) fft_queue(const __grid_constant__ QArgs a) {
+  constexpr int NCW = 16, NCT = NCW * 32, NMTMAX = 8;
+  constexpr int TMEM_COLS = SPLIT ? 128 : 256;
   using Q = QueueSmem;
   extern __shared__ uint8_t smem[];
   const uint32_t base_u = sm100::smem_u32(smem);
@@ -195,9 +230,10 @@ __global__ void __maxnreg__(96) fft_queue_f16(const __grid_constant__ QArgs a) {
   }
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + Q::OFF_BAR);  // [2]
   uint64_t* outrdy = full + 2;                                      // [2]
-  uint64_t* mmab = full + 4;                                        // [NMT]
+  uint64_t* mmab = full + 4;                                        // [up to 16]
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(full + 4 + 16);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(full + 4 + 17);
+  uint32_t* red = reinterpret_cast<uint32_t*>(full + 4 + 18);       // [2] split: tile maxima
   const int tid = threadIdx.x;
   const int warp = tid >> 5, lane = tid & 31;
   const bool producer = warp == NCW;
@@ -210,16 +246,20 @@ __global__ void __maxnreg__(96) fft_queue_f16(const __grid_constant__ QArgs a) {
       sm100::mbar_init(&full[1], 1);
       sm100::mbar_init(&outrdy[0], 1);
       sm100::mbar_init(&outrdy[1], 1);
-      for (int m = 0; m < NMT; ++m) sm100::mbar_init(&mmab[m], 1);
+      for (int m = 0; m < NMTMAX; ++m) sm100::mbar_init(&mmab[m], 1);
       *abort_flag = 0;
+      red[0] = 0u;
+      red[1] = 0u;
       sm100::fence_mbar_init();
     }
     __syncwarp();
     sm100::tmem_alloc(tmem_slot, TMEM_COLS);
     sm100::tmem_relinquish();
   } else {
-    for (int i = tid; i < 128; i += NCT)
+    for (int i = tid; i < 128; i += NCT) {
       *reinterpret_cast<uint4*>(smem + Q::OFF_B + 16 * i) = __ldg(a.bmat + i);
+      if (SPLIT) *reinterpret_cast<uint4*>(smem + Q::OFF_B + 2048 + 16 * i) = __ldg(a.bmat_lo + i);
+    }
   }
   sm100::fence_proxy_async_smem();
   sm100::tc_fence_before();
@@ -228,6 +268,7 @@ __global__ void __maxnreg__(96) fft_queue_f16(const __grid_constant__ QArgs a) {
   const uint32_t tmem_base = *tmem_slot;
   const TileCtx x{sS0, sS1, sA, base_u + Q::OFF_B, base_u + Q::OFF_TAIL, base_u + Q::OFF_TWS,
                   bS0, bS1, bA, tmem_base, mmab, abort_flag};
+  const SplitCtx xs{x, base_u + Q::OFF_B + 2048, red};
 
   if (producer) {
     // ------------------------------------------------------------- producer
@@ -315,21 +356,40 @@ __global__ void __maxnreg__(96) fft_queue_f16(const __grid_constant__ QArgs a) {
       if (!sm100::mbar_wait_bounded(&full[k & 1], (uint32_t)(k >> 1) & 1u, kWaitLimit)) *abort_flag = 1;
       if (*abort_flag) break;
       const uint32_t pi = a.items[blockIdx.x + k * G].pass;
-      switch (a.pass[pi].variant) {
-#define MCFFT_QCASE(V)                                                                   \
-  case V:                                                                                \
+      if constexpr (SPLIT) {
+        switch (a.pass[pi].variant) {
+#define MCFFT_QCASE(V)                                                                          \
+  case V:                                                                                       \
+    k = queue::run_variant_split<V>(a, pi, xs, smem, full, outrdy, tid, k, nlocal, mphase); \
+    break;
+          MCFFT_QCASE(0) MCFFT_QCASE(1) MCFFT_QCASE(2) MCFFT_QCASE(3)
+          MCFFT_QCASE(4) MCFFT_QCASE(5) MCFFT_QCASE(6) MCFFT_QCASE(7)
+          MCFFT_QCASE(8) MCFFT_QCASE(9) MCFFT_QCASE(10) MCFFT_QCASE(11)
+          MCFFT_QCASE(12) MCFFT_QCASE(13)
+          MCFFT_QCASE(16) MCFFT_QCASE(17) MCFFT_QCASE(18) MCFFT_QCASE(19)
+          MCFFT_QCASE(20) MCFFT_QCASE(21) MCFFT_QCASE(22) MCFFT_QCASE(23)
+          MCFFT_QCASE(24) MCFFT_QCASE(25) MCFFT_QCASE(26) MCFFT_QCASE(27)
+          MCFFT_QCASE(28) MCFFT_QCASE(29)
+#undef MCFFT_QCASE
+          default: *abort_flag = 1; break;
+        }
+      } else {
+        switch (a.pass[pi].variant) {
+#define MCFFT_QCASE(V)                                                                 \
+  case V:                                                                              \
     k = queue::run_variant<V>(a, pi, x, smem, full, outrdy, tid, k, nlocal, mphase); \
     break;
-        MCFFT_QCASE(0) MCFFT_QCASE(1) MCFFT_QCASE(2) MCFFT_QCASE(3)
-        MCFFT_QCASE(16) MCFFT_QCASE(17)
-        MCFFT_QCASE(4) MCFFT_QCASE(5) MCFFT_QCASE(6) MCFFT_QCASE(7)
-        MCFFT_QCASE(8) MCFFT_QCASE(9) MCFFT_QCASE(10) MCFFT_QCASE(11)
-        MCFFT_QCASE(12) MCFFT_QCASE(13) MCFFT_QCASE(14) MCFFT_QCASE(15)
-        MCFFT_QCASE(18) MCFFT_QCASE(19) MCFFT_QCASE(20) MCFFT_QCASE(21)
-        MCFFT_QCASE(22) MCFFT_QCASE(23) MCFFT_QCASE(24) MCFFT_QCASE(25)
-        MCFFT_QCASE(26) MCFFT_QCASE(27) MCFFT_QCASE(28) MCFFT_QCASE(29)
+          MCFFT_QCASE(0) MCFFT_QCASE(1) MCFFT_QCASE(2) MCFFT_QCASE(3)
+          MCFFT_QCASE(4) MCFFT_QCASE(5) MCFFT_QCASE(6) MCFFT_QCASE(7)
+          MCFFT_QCASE(8) MCFFT_QCASE(9) MCFFT_QCASE(10) MCFFT_QCASE(11)
+          MCFFT_QCASE(12) MCFFT_QCASE(13) MCFFT_QCASE(14) MCFFT_QCASE(15)
+          MCFFT_QCASE(16) MCFFT_QCASE(17)
+          MCFFT_QCASE(18) MCFFT_QCASE(19) MCFFT_QCASE(20) MCFFT_QCASE(21)
+          MCFFT_QCASE(22) MCFFT_QCASE(23) MCFFT_QCASE(24) MCFFT_QCASE(25)
+          MCFFT_QCASE(26) MCFFT_QCASE(27) MCFFT_QCASE(28) MCFFT_QCASE(29)
 #undef MCFFT_QCASE
-        default: *abort_flag = 1; break;
+          default: *abort_flag = 1; break;
+        }
       }
       if (*abort_flag) break;
     }

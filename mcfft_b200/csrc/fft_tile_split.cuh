@@ -100,24 +100,322 @@ __device__ __forceinline__ float2 load_point(const uint4& q, int i) {
   }
 }
 
+// Split-form handles: the plain ones plus the low DFT matrix and the
+// per-tile maximum slots.
+struct SplitCtx {
+  TileCtx t;       // sB = high DFT-16 matrix
+  uint32_t sBl;    // low DFT-16 matrix
+  uint32_t* red;   // [2] tile maxima (uint bits of a non-negative float)
+};
+
+// One tile of one pass, split form (see the file comment), run by the NCW
+// consumer warps once the tile's staging buffer b holds its input; k is
+// the CTA-local tile index (its parity picks the maximum slot).  `A` is any
+// argument block with the pass's tables (TileArgs, or a pass of the batch
+// queue).
+template <int L, int R, int C, bool POSTTW, int NCW, bool IN16>
+struct SplitTile {
+  using S = TileShape<L, R, C, NCW>;
+  using T = TileSplit<L, R, C, POSTTW, NCW, IN16>;
+  static constexpr int NCT = S::NCT;
+  static constexpr int NH = IN16 ? 1 : 2;               // loads per point group
+  static constexpr int SUBV = 4 / NH;                   // sub-vectors per prologue unit
+  static constexpr int UNITS = S::ITEMS * NH;
+  static constexpr int NIT_P = (UNITS + NCT - 1) / NCT;  // prologue units per consumer thread
+  static constexpr int NLD = R == 1 ? 4 : R;            // 16-byte loads per unit
+  static constexpr int NIT_E = S::NMT * 4 / NCW;
+  static constexpr int NMT = S::NMT;
+  static constexpr int NST = S::NST;
+  static constexpr int TMEM_COLS = S::TMEM_COLS;
+  static_assert(S::NMT * 4 % NCW == 0, "row blocks per warp");
+  static_assert(NMT <= 16, "per-M-tile barriers");
+  static_assert(NIT_P * NLD <= 8, "prologue registers");
+  static constexpr bool INPLACE_PROLOGUE = (S::NST % 2) == 0;
+  static constexpr int LGL = ilog2c(L);
+
+  template <class A>
+  static __device__ __forceinline__ void entries(const A& a, int ctid, uint2 (&ient)[NIT_P],
+                                                 uint32_t (&eent)[NST][NIT_E]) {
+    const int warp = ctid >> 5, lane = ctid & 31, sp = warp & 3;
+#pragma unroll
+    for (int j = 0; j < NIT_P; ++j) {
+      const int u = ctid + j * NCT;
+      ient[j] = u < UNITS ? __ldg(a.item_tab + (u % S::ITEMS)) : make_uint2(0u, 0u);
+    }
+#pragma unroll
+    for (int s = 0; s < NST; ++s)
+#pragma unroll
+      for (int j = 0; j < NIT_E; ++j) {
+        const uint32_t m = (warp >> 2) + j * (NCW / 4);
+        eent[s][j] = __ldg(a.epi_tab + s * S::NROWS + m * 128 + sp * 32 + lane);
+      }
+  }
+
+  // Radix-R twiddles (FP32, 1/R) and stage twiddle rows into shared memory;
+  // consumer threads only.
+  template <class A>
+  static __device__ __forceinline__ void tables(const A& a, uint8_t* tail, uint8_t* tws, int ctid) {
+    if constexpr (R > 1) {
+      for (int i = ctid; i < L; i += NCT)
+        *reinterpret_cast<float2*>(tail + 8 * i) = __ldg(a.tail_tw + i);
+    }
+    if constexpr (T::TW_SMEM && T::TW_ROWS > 0) {
+      for (int i = ctid; i < T::TW_ROWS * 8; i += NCT)
+        *reinterpret_cast<float4*>(tws + 16 * i) = __ldg(a.tw + i);
+    }
+  }
+
+  template <class A>
+  static __device__ __forceinline__ void run(const A& a, const SplitCtx& x, int ctid, int b,
+                                             int64_t cb, int64_t k, uint32_t& mphase,
+                                             const uint2 (&ient)[NIT_P],
+                                             const uint32_t (&eent)[NST][NIT_E]) {
+    const int warp = ctid >> 5, lane = ctid & 31, sp = warp & 3;
+    constexpr uint32_t IDESC = sm100::idesc_f16_f32(128, 32);
+    const float tsgn = a.inverse ? 1.f : -1.f;
+    const uint32_t sb = b ? x.t.sS1 : x.t.sS0;
+    const uint32_t bb = b ? x.t.bS1 : x.t.bS0;
+    // A pass with fewer columns than C loads only its own column blocks,
+    // the leading part of the staging buffer; zero the rest so that stale
+    // data does not enter the tile maximum.
+    constexpr uint32_t kInBytes = (uint32_t)T::TP * (IN16 ? 4 : 8);
+    if (a.in_tile_bytes < kInBytes) {
+      for (uint32_t o = a.in_tile_bytes + 16u * ctid; o < kInBytes; o += 16u * NCT)
+        sts128w(bb + o, make_uint4(0u, 0u, 0u, 0u));
+      tile::named_bar(1, NCT);
+    }
+    // ------------------------------------------- tile maximum and scale
+    uint4 q[NIT_P][NLD];
+    {
+      uint32_t amax = 0;
+#pragma unroll
+      for (int j = 0; j < NIT_P; ++j) {
+        const int u = ctid + j * NCT;
+        const uint32_t h = (uint32_t)(u / S::ITEMS);
+        const uint32_t lb = (ient[j].x & 0xFFFFu) << 2;
+#pragma unroll
+        for (int n = 0; n < NLD; ++n) {
+          q[j][n] = u < UNITS ? lds128w(xo(lb, a.lofs[n * NH + h], bb)) : make_uint4(0u, 0u, 0u, 0u);
+#pragma unroll
+          for (int pp = 0; pp < 4 / NH; ++pp) {
+            const float2 x = load_point<IN16>(q[j][n], pp);
+            amax = max(amax, __float_as_uint(fabsf(x.x)));
+            amax = max(amax, __float_as_uint(fabsf(x.y)));
+          }
+        }
+      }
+      amax = __reduce_max_sync(0xffffffffu, amax);
+      if (lane == 0) atomicMax(&x.red[k & 1], amax);
+    }
+    tile::named_bar(1, NCT);
+    const uint32_t tmax = x.red[k & 1];
+    if (ctid == 0) x.red[(k + 1) & 1] = 0u;  // next tile's slot; last read a tile ago
+    // 2^sexp puts the tile maximum in [2^13, 2^14)
+    const int sexp = tmax == 0 ? 0 : 13 - ((int)((tmax >> 23) & 0xff) - 127);
+    const float sc = exp2i(sexp);
+    // L / (16 2^sexp): undoes the stage scalings (1/L in total) and the tile scale
+    const float fm = exp2i(LGL - 4 - sexp);
+
+    // ---------------------------------------------------------- prologue
+    const uint32_t x0 = INPLACE_PROLOGUE ? bb : x.t.bA;  // stage-0 operand (hi; lo at + HALF)
+    const uint32_t x0l = x0 + T::HALF;
+    // The maximum pass already holds every unit's loads in q; staging is
+    // rewritten in place only after all consumers are past the barrier
+    // above, which they are.
+#pragma unroll
+    for (int j = 0; j < NIT_P; ++j) {
+      const int u = ctid + j * NCT;
+      if (UNITS % NCT != 0 && u >= UNITS) break;
+      const uint32_t h = (uint32_t)(u / S::ITEMS);
+      const uint32_t st = (ient[j].x >> 16) << 2;
+      if constexpr (R == 1) {
+#pragma unroll
+        for (int jj = 0; jj < SUBV; ++jj) {
+          const int sv = SUBV * h + jj;  // sub-vector within the item
+          uint32_t hi[4], lo[4];
+#pragma unroll
+          for (int n = 0; n < 4; ++n) {
+            const float2 x = load_point<IN16>(q[j][n], jj);
+            split2(make_float2(x.x * sc, x.y * sc), hi[n], lo[n]);
+          }
+          sts128w(xo(st, a.sofs[sv], x0), make_uint4(hi[0], hi[1], hi[2], hi[3]));
+          sts128w(xo(st, a.sofs[sv], x0l), make_uint4(lo[0], lo[1], lo[2], lo[3]));
+        }
+      } else {
+        const uint32_t trow = ient[j].y & 0x7FFFFFFFu;
+        const bool colitem = (ient[j].y >> 31) != 0;
+        // Sub-vector jj of the unit: radix-R butterflies, twiddle times
+        // the tile scale, split, stores.
+        auto subvec = [&](int jj, auto tw_of) {
+          const int sv = SUBV * h + jj;
+          float2 x[R];
+#pragma unroll
+          for (int n = 0; n < R; ++n) x[n] = load_point<IN16>(q[j][n], jj);
+          small_dft<R>(x, tsgn);
+#pragma unroll
+          for (int k = 0; k < R; ++k) {
+            uint32_t hi, lo;
+            split2(cmulf(x[k], tw_of(k)), hi, lo);
+            sts32w(xo(st, a.sofs[sv * R + k], x0), hi);
+            sts32w(xo(st, a.sofs[sv * R + k], x0l), lo);
+          }
+        };
+        if (colitem) {
+          // column items: the sub-vectors share one twiddle row
+          float2 wc[R];
+#pragma unroll
+          for (int k = 0; k < R; ++k) {
+            const float2 w = lds64f(x.t.sTail + (trow * R + k) * 8);
+            wc[k] = make_float2(w.x * sc, w.y * sc);
+          }
+#pragma unroll
+          for (int jj = 0; jj < SUBV; ++jj) subvec(jj, [&](int k) { return wc[k]; });
+        } else {
+#pragma unroll
+          for (int jj = 0; jj < SUBV; ++jj)
+            subvec(jj, [&](int k) {
+              const float2 w = lds64f(x.t.sTail + ((trow + SUBV * h + jj) * R + k) * 8);
+              return make_float2(w.x * sc, w.y * sc);
+            });
+        }
+      }
+    }
+    sm100::fence_proxy_async_smem();
+    sm100::tc_fence_before();
+    tile::named_bar(1, NCT);
+    sm100::tc_fence_after();
+
+    // ------------------------------------------------------------ stages
+#pragma unroll
+    for (int s = 0; s < S::NST; ++s) {
+      const uint32_t xs = ((S::NST - s) & 1) ? x.t.sA : sb;   // this stage's operand (hi)
+      const uint32_t xn = ((S::NST - s) & 1) ? bb : x.t.bA;   // next stage's operand (window-relative)
+      const uint32_t xnl = xn + T::HALF;
+      if (sp == 0 && lane == 0) {
+#pragma unroll
+        for (int j = 0; j < NIT_E; ++j) {
+          const uint32_t m = (warp >> 2) + j * (NCW / 4);
+          const uint32_t d = x.t.tmem + 32u * m;
+#pragma unroll
+          for (int ks = 0; ks < 2; ++ks) {
+            const uint64_t ah = tile::sdesc_sw64(xs + m * 8192u + ks * 32u);
+            const uint64_t al = tile::sdesc_sw64(xs + T::HALF + m * 8192u + ks * 32u);
+            const uint64_t bh = tile::sdesc_sw64(x.t.sB + ks * 32u);
+            const uint64_t bl = tile::sdesc_sw64(x.sBl + ks * 32u);
+            sm100::umma_f16(d, ah, bh, IDESC, ks);
+            sm100::umma_f16(d, al, bh, IDESC, 1);
+            sm100::umma_f16(d, ah, bl, IDESC, 1);
+          }
+          sm100::umma_commit(&x.t.mmab[m]);
+        }
+      }
+      const bool last = s == S::NST - 1;
+      const uint32_t row0 = stage_tw_row0<L, R>(s);
+      float2 pt[NIT_E][2];
+      if (POSTTW && last) post_twiddles<C, S::NV>(a, cb, s, eent, pt);
+#pragma unroll
+      for (int j = 0; j < NIT_E; ++j) {
+        const uint32_t m = (warp >> 2) + j * (NCW / 4);
+        const uint32_t e = eent[s][j];
+        const uint32_t aux = e >> 16;
+        const uint32_t dst = (e & 0xFFFFu) << 2;
+        float4 wg[8];
+        if (!last && !T::TW_SMEM) {
+          const float4* t4 = a.tw + (size_t)(row0 + aux) * 8;
+#pragma unroll
+          for (int p = 0; p < 8; ++p) wg[p] = __ldg(t4 + (p ^ tw_fold(aux)));
+        }
+        if (!sm100::mbar_wait_bounded(&x.t.mmab[m], (mphase >> m) & 1u, kWaitLimit)) *x.t.abort_flag = 1;
+        sm100::tc_fence_after();
+        uint32_t d[32];
+        sm100::tmem_ld32(x.t.tmem + ((uint32_t)(32 * sp) << 16) + 32u * m, d);
+        if (!last) {
+          const uint32_t trow = x.t.sTws + (row0 + aux) * 128u;
+          const uint32_t fold = tw_fold(aux);
+          sm100::tmem_wait_ld();
+#pragma unroll
+          for (int hh = 0; hh < 2; ++hh) {
+            float4 w[4];
+#pragma unroll
+            for (int pp = 0; pp < 4; ++pp)
+              w[pp] = T::TW_SMEM ? lds128f(trow + (((4 * hh + pp) ^ fold) << 4)) : wg[4 * hh + pp];
+#pragma unroll
+            for (int pp = 0; pp < 4; ++pp) {
+              const int p = 4 * hh + pp;
+              uint64_t yr, yi;
+              cmul2(f2p(__uint_as_float(d[4 * p]), __uint_as_float(d[4 * p + 1])),
+                    f2p(__uint_as_float(d[4 * p + 2]), __uint_as_float(d[4 * p + 3])),
+                    f2p(w[pp].x, w[pp].y), f2p(w[pp].z, w[pp].w), yr, yi);
+              uint32_t h0, h1, l0, l1;
+              split_pair(yr, yi, h0, h1, l0, l1);
+              sts32w(xo(dst, a.kofs[s][2 * p], xn), h0);
+              sts32w(xo(dst, a.kofs[s][2 * p], xnl), l0);
+              sts32w(xo(dst, a.kofs[s][2 * p + 1], xn), h1);
+              sts32w(xo(dst, a.kofs[s][2 * p + 1], xnl), l1);
+            }
+          }
+        } else if (POSTTW) {
+          // Four-step twiddle W_N^((v + NV k) g) times L / (16 2^sexp):
+          // pairs (w_2p, w_2p+1) advanced by ws^2 (FP32 recurrence, 7
+          // steps, ~1e-7 relative).
+          float2 w0 = pt[j][0];
+          const float2 ws = pt[j][1];
+          w0.x *= fm;
+          w0.y *= fm;
+          const float2 w1 = cmulf(w0, ws);
+          const float2 s2 = cmulf(ws, ws);
+          uint64_t wr = f2p(w0.x, w1.x), wi = f2p(w0.y, w1.y);
+          const uint64_t s2r = f2p(s2.x, s2.x), s2i = f2p(s2.y, s2.y);
+          sm100::tmem_wait_ld();
+#pragma unroll
+          for (int p = 0; p < 8; ++p) {
+            uint64_t yr, yi;
+            cmul2(f2p(__uint_as_float(d[4 * p]), __uint_as_float(d[4 * p + 1])),
+                  f2p(__uint_as_float(d[4 * p + 2]), __uint_as_float(d[4 * p + 3])), wr, wi, yr,
+                  yi);
+            float r0, r1, i0, i1;
+            f2u(yr, r0, r1);
+            f2u(yi, i0, i1);
+            sts64w(xo(dst, a.kofs[s][2 * p], bb), r0, i0);
+            sts64w(xo(dst, a.kofs[s][2 * p + 1], bb), r1, i1);
+            if (p < 7) {
+              uint64_t nr, ni;
+              cmul2(wr, wi, s2r, s2i, nr, ni);
+              wr = nr;
+              wi = ni;
+            }
+          }
+        } else {
+          sm100::tmem_wait_ld();
+          const uint64_t fm2 = f2p(fm, fm);
+#pragma unroll
+          for (int p = 0; p < 8; ++p) {
+            float r0, r1, i0, i1;
+            f2u(mul2(f2p(__uint_as_float(d[4 * p]), __uint_as_float(d[4 * p + 1])), fm2), r0, r1);
+            f2u(mul2(f2p(__uint_as_float(d[4 * p + 2]), __uint_as_float(d[4 * p + 3])), fm2), i0, i1);
+            sts64w(xo(dst, a.kofs[s][2 * p], bb), r0, i0);
+            sts64w(xo(dst, a.kofs[s][2 * p + 1], bb), r1, i1);
+          }
+        }
+      }
+      mphase ^= (1u << NMT) - 1u;
+      sm100::fence_proxy_async_smem();
+      sm100::tc_fence_before();
+      tile::named_bar(1, NCT);
+      sm100::tc_fence_after();
+      if (*x.t.abort_flag) break;
+    }
+  }
+};
+
 template <int L, int R, int C, bool POSTTW, int NCW, bool IN16>
 // 17 warps are granted registers as 20: 65536 / 640 -> 96 per thread.
 __global__ void __maxnreg__(96) fft_tile_split(const __grid_constant__ TileArgs a) {
   using S = TileShape<L, R, C, NCW>;
   using T = TileSplit<L, R, C, POSTTW, NCW, IN16>;
+  using TL = SplitTile<L, R, C, POSTTW, NCW, IN16>;
   constexpr int NCT = S::NCT;
-  constexpr int NH = IN16 ? 1 : 2;               // loads per point group
-  constexpr int SUBV = 4 / NH;                   // sub-vectors per prologue unit
-  constexpr int UNITS = S::ITEMS * NH;
-  constexpr int NIT_P = (UNITS + NCT - 1) / NCT;  // prologue units per consumer thread
-  constexpr int NLD = R == 1 ? 4 : R;            // 16-byte loads per unit
-  constexpr int NIT_E = S::NMT * 4 / NCW;
   constexpr int NMT = S::NMT;
-  static_assert(S::NMT * 4 % NCW == 0, "row blocks per warp");
-  static_assert(NMT <= 16, "per-M-tile barriers");
-  static_assert(NIT_P * NLD <= 8, "prologue registers");
-  constexpr bool INPLACE_PROLOGUE = (S::NST % 2) == 0;
-  constexpr int LGL = ilog2c(L);
   extern __shared__ uint8_t smem_raw[];
   const uint32_t raw_u = sm100::smem_u32(smem_raw);
   const uint32_t base_u = (raw_u + 1023u) & ~1023u;
@@ -162,20 +460,15 @@ __global__ void __maxnreg__(96) fft_tile_split(const __grid_constant__ TileArgs 
       *reinterpret_cast<uint4*>(smem + T::OFF_B + 16 * i) = __ldg(a.bmat + i);
       *reinterpret_cast<uint4*>(smem + T::OFF_B + 2048 + 16 * i) = __ldg(a.bmat_lo + i);
     }
-    if constexpr (R > 1) {
-      for (int i = tid; i < L; i += NCT)
-        *reinterpret_cast<float2*>(smem + T::OFF_TAIL + 8 * i) = __ldg(a.tail_tw + i);
-    }
-    if constexpr (T::TW_SMEM && T::TW_ROWS > 0) {
-      for (int i = tid; i < T::TW_ROWS * 8; i += NCT)
-        *reinterpret_cast<float4*>(smem + T::OFF_TWS + 16 * i) = __ldg(a.tw + i);
-    }
+    TL::tables(a, smem + T::OFF_TAIL, smem + T::OFF_TWS, tid);
   }
   sm100::fence_proxy_async_smem();
   sm100::tc_fence_before();
   __syncthreads();
   sm100::tc_fence_after();
   const uint32_t tmem_base = *tmem_slot;
+  const SplitCtx x{{sS0, sS1, sA, sBh, sTail, sTws, bS0, bS1, bA, tmem_base, mmab, abort_flag},
+                   sBl, red};
 
   if (producer) {
     // ------------------------------------------------------------- producer
@@ -222,259 +515,18 @@ __global__ void __maxnreg__(96) fft_tile_split(const __grid_constant__ TileArgs 
     __syncwarp();
   } else {
     // ------------------------------------------------------------ consumers
-    const int ctid = tid;
-    const int sp = warp & 3;
-    constexpr uint32_t IDESC = sm100::idesc_f16_f32(128, 32);
-    uint32_t mphase = 0;
-    const float tsgn = a.inverse ? 1.f : -1.f;
-
-    uint2 ient[NIT_P];
-#pragma unroll
-    for (int j = 0; j < NIT_P; ++j) {
-      const int u = ctid + j * NCT;
-      ient[j] = u < UNITS ? __ldg(a.item_tab + (u % S::ITEMS)) : make_uint2(0u, 0u);
-    }
-    uint32_t eent[S::NST][NIT_E];
-#pragma unroll
-    for (int s = 0; s < S::NST; ++s)
-#pragma unroll
-      for (int j = 0; j < NIT_E; ++j) {
-        const uint32_t m = (warp >> 2) + j * (NCW / 4);
-        eent[s][j] = __ldg(a.epi_tab + s * S::NROWS + m * 128 + sp * 32 + lane);
-      }
-
+    uint2 ient[TL::NIT_P];
+    uint32_t eent[TL::NST][TL::NIT_E];
+    TL::entries(a, tid, ient, eent);
+    uint32_t mphase = 0;  // bit m: completions of M-tile barrier m so far, mod 2
     int i = 0;
     for (int64_t t = blockIdx.x; t < a.ntiles; t += gridDim.x, ++i) {
       const int b = i & 1;
-      const uint32_t sb = b ? sS1 : sS0;
-      const uint32_t bb = b ? bS1 : bS0;
-      const int64_t cb = t % a.col_blocks;
       if (!sm100::mbar_wait_bounded(&full[b], (i >> 1) & 1, kWaitLimit)) *abort_flag = 1;
       if (*abort_flag) break;
-
-      // ------------------------------------------- tile maximum and scale
-      uint4 q[NIT_P][NLD];
-      {
-        uint32_t amax = 0;
-#pragma unroll
-        for (int j = 0; j < NIT_P; ++j) {
-          const int u = ctid + j * NCT;
-          const uint32_t h = (uint32_t)(u / S::ITEMS);
-          const uint32_t lb = (ient[j].x & 0xFFFFu) << 2;
-#pragma unroll
-          for (int n = 0; n < NLD; ++n) {
-            q[j][n] = u < UNITS ? lds128w(xo(lb, a.lofs[n * NH + h], bb)) : make_uint4(0u, 0u, 0u, 0u);
-#pragma unroll
-            for (int pp = 0; pp < 4 / NH; ++pp) {
-              const float2 x = load_point<IN16>(q[j][n], pp);
-              amax = max(amax, __float_as_uint(fabsf(x.x)));
-              amax = max(amax, __float_as_uint(fabsf(x.y)));
-            }
-          }
-        }
-        amax = __reduce_max_sync(0xffffffffu, amax);
-        if (lane == 0) atomicMax(&red[i & 1], amax);
-      }
-      tile::named_bar(1, NCT);
-      const uint32_t tmax = red[i & 1];
-      if (ctid == 0) red[(i + 1) & 1] = 0u;  // next tile's slot; last read a tile ago
-      // 2^sexp puts the tile maximum in [2^13, 2^14)
-      const int sexp = tmax == 0 ? 0 : 13 - ((int)((tmax >> 23) & 0xff) - 127);
-      const float sc = exp2i(sexp);
-      // L / (16 2^sexp): undoes the stage scalings (1/L in total) and the tile scale
-      const float fm = exp2i(LGL - 4 - sexp);
-
-      // ---------------------------------------------------------- prologue
-      const uint32_t x0 = INPLACE_PROLOGUE ? bb : bA;  // stage-0 operand (hi; lo at + HALF)
-      const uint32_t x0l = x0 + T::HALF;
-      // The maximum pass already holds every unit's loads in q; staging is
-      // rewritten in place only after all consumers are past the barrier
-      // above, which they are.
-#pragma unroll
-      for (int j = 0; j < NIT_P; ++j) {
-        const int u = ctid + j * NCT;
-        if (UNITS % NCT != 0 && u >= UNITS) break;
-        const uint32_t h = (uint32_t)(u / S::ITEMS);
-        const uint32_t st = (ient[j].x >> 16) << 2;
-        if constexpr (R == 1) {
-#pragma unroll
-          for (int jj = 0; jj < SUBV; ++jj) {
-            const int sv = SUBV * h + jj;  // sub-vector within the item
-            uint32_t hi[4], lo[4];
-#pragma unroll
-            for (int n = 0; n < 4; ++n) {
-              const float2 x = load_point<IN16>(q[j][n], jj);
-              split2(make_float2(x.x * sc, x.y * sc), hi[n], lo[n]);
-            }
-            sts128w(xo(st, a.sofs[sv], x0), make_uint4(hi[0], hi[1], hi[2], hi[3]));
-            sts128w(xo(st, a.sofs[sv], x0l), make_uint4(lo[0], lo[1], lo[2], lo[3]));
-          }
-        } else {
-          const uint32_t trow = ient[j].y & 0x7FFFFFFFu;
-          const bool colitem = (ient[j].y >> 31) != 0;
-          // Sub-vector jj of the unit: radix-R butterflies, twiddle times
-          // the tile scale, split, stores.
-          auto subvec = [&](int jj, auto tw_of) {
-            const int sv = SUBV * h + jj;
-            float2 x[R];
-#pragma unroll
-            for (int n = 0; n < R; ++n) x[n] = load_point<IN16>(q[j][n], jj);
-            small_dft<R>(x, tsgn);
-#pragma unroll
-            for (int k = 0; k < R; ++k) {
-              uint32_t hi, lo;
-              split2(cmulf(x[k], tw_of(k)), hi, lo);
-              sts32w(xo(st, a.sofs[sv * R + k], x0), hi);
-              sts32w(xo(st, a.sofs[sv * R + k], x0l), lo);
-            }
-          };
-          if (colitem) {
-            // column items: the sub-vectors share one twiddle row
-            float2 wc[R];
-#pragma unroll
-            for (int k = 0; k < R; ++k) {
-              const float2 w = lds64f(sTail + (trow * R + k) * 8);
-              wc[k] = make_float2(w.x * sc, w.y * sc);
-            }
-#pragma unroll
-            for (int jj = 0; jj < SUBV; ++jj) subvec(jj, [&](int k) { return wc[k]; });
-          } else {
-#pragma unroll
-            for (int jj = 0; jj < SUBV; ++jj)
-              subvec(jj, [&](int k) {
-                const float2 w = lds64f(sTail + ((trow + SUBV * h + jj) * R + k) * 8);
-                return make_float2(w.x * sc, w.y * sc);
-              });
-          }
-        }
-      }
-      sm100::fence_proxy_async_smem();
-      sm100::tc_fence_before();
-      tile::named_bar(1, NCT);
-      sm100::tc_fence_after();
-
-      // ------------------------------------------------------------ stages
-#pragma unroll
-      for (int s = 0; s < S::NST; ++s) {
-        const uint32_t xs = ((S::NST - s) & 1) ? sA : sb;   // this stage's operand (hi)
-        const uint32_t xn = ((S::NST - s) & 1) ? bb : bA;   // next stage's operand (window-relative)
-        const uint32_t xnl = xn + T::HALF;
-        if (sp == 0 && lane == 0) {
-#pragma unroll
-          for (int j = 0; j < NIT_E; ++j) {
-            const uint32_t m = (warp >> 2) + j * (NCW / 4);
-            const uint32_t d = tmem_base + 32u * m;
-#pragma unroll
-            for (int ks = 0; ks < 2; ++ks) {
-              const uint64_t ah = tile::sdesc_sw64(xs + m * 8192u + ks * 32u);
-              const uint64_t al = tile::sdesc_sw64(xs + T::HALF + m * 8192u + ks * 32u);
-              const uint64_t bh = tile::sdesc_sw64(sBh + ks * 32u);
-              const uint64_t bl = tile::sdesc_sw64(sBl + ks * 32u);
-              sm100::umma_f16(d, ah, bh, IDESC, ks);
-              sm100::umma_f16(d, al, bh, IDESC, 1);
-              sm100::umma_f16(d, ah, bl, IDESC, 1);
-            }
-            sm100::umma_commit(&mmab[m]);
-          }
-        }
-        const bool last = s == S::NST - 1;
-        const uint32_t row0 = stage_tw_row0<L, R>(s);
-        float2 pt[NIT_E][2];
-        if (POSTTW && last) post_twiddles<C, S::NV>(a, cb, s, eent, pt);
-#pragma unroll
-        for (int j = 0; j < NIT_E; ++j) {
-          const uint32_t m = (warp >> 2) + j * (NCW / 4);
-          const uint32_t e = eent[s][j];
-          const uint32_t aux = e >> 16;
-          const uint32_t dst = (e & 0xFFFFu) << 2;
-          float4 wg[8];
-          if (!last && !T::TW_SMEM) {
-            const float4* t4 = a.tw + (size_t)(row0 + aux) * 8;
-#pragma unroll
-            for (int p = 0; p < 8; ++p) wg[p] = __ldg(t4 + (p ^ tw_fold(aux)));
-          }
-          if (!sm100::mbar_wait_bounded(&mmab[m], mphase, kWaitLimit)) *abort_flag = 1;
-          sm100::tc_fence_after();
-          uint32_t d[32];
-          sm100::tmem_ld32(tmem_base + ((uint32_t)(32 * sp) << 16) + 32u * m, d);
-          if (!last) {
-            const uint32_t trow = sTws + (row0 + aux) * 128u;
-            const uint32_t fold = tw_fold(aux);
-            sm100::tmem_wait_ld();
-#pragma unroll
-            for (int hh = 0; hh < 2; ++hh) {
-              float4 w[4];
-#pragma unroll
-              for (int pp = 0; pp < 4; ++pp)
-                w[pp] = T::TW_SMEM ? lds128f(trow + (((4 * hh + pp) ^ fold) << 4)) : wg[4 * hh + pp];
-#pragma unroll
-              for (int pp = 0; pp < 4; ++pp) {
-                const int p = 4 * hh + pp;
-                uint64_t yr, yi;
-                cmul2(f2p(__uint_as_float(d[4 * p]), __uint_as_float(d[4 * p + 1])),
-                      f2p(__uint_as_float(d[4 * p + 2]), __uint_as_float(d[4 * p + 3])),
-                      f2p(w[pp].x, w[pp].y), f2p(w[pp].z, w[pp].w), yr, yi);
-                uint32_t h0, h1, l0, l1;
-                split_pair(yr, yi, h0, h1, l0, l1);
-                sts32w(xo(dst, a.kofs[s][2 * p], xn), h0);
-                sts32w(xo(dst, a.kofs[s][2 * p], xnl), l0);
-                sts32w(xo(dst, a.kofs[s][2 * p + 1], xn), h1);
-                sts32w(xo(dst, a.kofs[s][2 * p + 1], xnl), l1);
-              }
-            }
-          } else if (POSTTW) {
-            // Four-step twiddle W_N^((v + NV k) g) times L / (16 2^sexp):
-            // pairs (w_2p, w_2p+1) advanced by ws^2 (FP32 recurrence, 7
-            // steps, ~1e-7 relative).
-            float2 w0 = pt[j][0];
-            const float2 ws = pt[j][1];
-            w0.x *= fm;
-            w0.y *= fm;
-            const float2 w1 = cmulf(w0, ws);
-            const float2 s2 = cmulf(ws, ws);
-            uint64_t wr = f2p(w0.x, w1.x), wi = f2p(w0.y, w1.y);
-            const uint64_t s2r = f2p(s2.x, s2.x), s2i = f2p(s2.y, s2.y);
-            sm100::tmem_wait_ld();
-#pragma unroll
-            for (int p = 0; p < 8; ++p) {
-              uint64_t yr, yi;
-              cmul2(f2p(__uint_as_float(d[4 * p]), __uint_as_float(d[4 * p + 1])),
-                    f2p(__uint_as_float(d[4 * p + 2]), __uint_as_float(d[4 * p + 3])), wr, wi, yr,
-                    yi);
-              float r0, r1, i0, i1;
-              f2u(yr, r0, r1);
-              f2u(yi, i0, i1);
-              sts64w(xo(dst, a.kofs[s][2 * p], bb), r0, i0);
-              sts64w(xo(dst, a.kofs[s][2 * p + 1], bb), r1, i1);
-              if (p < 7) {
-                uint64_t nr, ni;
-                cmul2(wr, wi, s2r, s2i, nr, ni);
-                wr = nr;
-                wi = ni;
-              }
-            }
-          } else {
-            sm100::tmem_wait_ld();
-            const uint64_t fm2 = f2p(fm, fm);
-#pragma unroll
-            for (int p = 0; p < 8; ++p) {
-              float r0, r1, i0, i1;
-              f2u(mul2(f2p(__uint_as_float(d[4 * p]), __uint_as_float(d[4 * p + 1])), fm2), r0, r1);
-              f2u(mul2(f2p(__uint_as_float(d[4 * p + 2]), __uint_as_float(d[4 * p + 3])), fm2), i0, i1);
-              sts64w(xo(dst, a.kofs[s][2 * p], bb), r0, i0);
-              sts64w(xo(dst, a.kofs[s][2 * p + 1], bb), r1, i1);
-            }
-          }
-        }
-        mphase ^= 1u;
-        sm100::fence_proxy_async_smem();
-        sm100::tc_fence_before();
-        tile::named_bar(1, NCT);
-        sm100::tc_fence_after();
-        if (*abort_flag) break;
-      }
+      TL::run(a, x, tid, b, t % a.col_blocks, i, mphase, ient, eent);
       if (*abort_flag) break;
-      if (ctid == 0) tile::mbar_arrive(&outrdy[b]);
+      if (tid == 0) tile::mbar_arrive(&outrdy[b]);
     }
   }
   __syncthreads();

@@ -7,8 +7,8 @@
 // length-L transform (L = 16^a * R) along one axis, and picks a tile shape
 // for each pass from the instantiated kernel variants.
 //
-//   1D, n <= 4096        one row pass
-//   1D, n > 4096         four-step: n = n1 * n2; pass 1 = n1-point column
+//   1D, n <= 4096        one row pass (split form: n <= 2048)
+//   1D, larger n         four-step: n = n1 * n2; pass 1 = n1-point column
 //                        transforms (stride n2) with the W_n^(k1 n2)
 //                        twiddle fused into their epilogue, into a scratch
 //                        buffer; pass 2 = n2-point row transforms written
@@ -273,9 +273,6 @@ mcfftResult add_tile_pass(mcfftPlan p, const PassSpec& s) {
     if (!tile_layout(&tp.lay, cand->L, cand->R, cand->C, ik, ok, in_elem, out_elem, s.in_sp,
                      s.in_sc, s.in_so, s.out_sp, s.out_sc, s.out_so, s.ncols, s.nouter, &err))
       continue;
-    // the split form's tile maximum must not see the stale columns of a
-    // clamped tile
-    if (p->split && (tp.lay.in.clamped() || tp.lay.out.clamped())) continue;
     if (!tile_check_encode(tp.lay.in, p->status) || !tile_check_encode(tp.lay.out, p->status))
       continue;
     k = cand;
@@ -427,7 +424,7 @@ mcfftResult add_pass(mcfftPlan p, const PassSpec& s) {
 }
 
 constexpr int64_t kMaxSinglePass = 8192;
-constexpr int64_t kMaxTilePass = 4096;  // 1D lengths above run as four-step
+constexpr int64_t kMaxTilePass = 4096;  // 1D lengths above run as four-step (split: 2048)
 
 // Appends the passes of one transform group.  `in_buf/out_buf` and offsets
 // locate it inside the user's buffers; the first pass reads in_buf, the
@@ -445,7 +442,8 @@ mcfftResult build_group_passes(mcfftPlan p, int ndim, const int64_t* dims, int64
   *scale_log2 = split ? 0 : -ilog2(total);
   if (ndim == 1) {
     const int64_t n = dims[0];
-    if (n <= kMaxTilePass) {
+    // the split tile kernel's 8K-point tiles hold at most L = 2048
+    if (n <= (split ? kMaxTilePass / 2 : kMaxTilePass)) {
       PassSpec s{n, false, false, 1, n, 0, 1, n, 0, batch, 1, kUserIn, kUserOut, 0,
                  in_f16, split ? 0 : 1, in_off, out_off};
       return add_pass(p, s);
@@ -600,10 +598,10 @@ mcfftResult build_group(mcfftPlan p, int ndim, const int64_t* dims, int64_t batc
 // Builds the batch queue (every pass of the plan in one persistent launch)
 // for plans of several transform groups (uneven batches) -- or any plan
 // with MCFFT_QUEUE=1; MCFFT_QUEUE=0 disables it -- when every pass runs on
-// the 16K-point plain tile kernel and the passes fit the kernel's parameter
-// block; otherwise the plan launches pass by pass (one transform shape is
-// faster that way: each pass kernel keeps its tables in its parameter
-// block).
+// a tile-kernel variant the batch kernel holds and the passes fit its
+// parameter block; otherwise the plan launches pass by pass (one transform
+// shape is faster that way: each pass kernel keeps its tables in its
+// parameter block).
 // Queue order: per transform group, the first pass's tiles in chunks of
 // four per CTA, each later pass's tile for key k once the previous pass's
 // tiles for keys up to k + W are queued (W ~ four tiles per CTA of lag), so
@@ -611,21 +609,19 @@ mcfftResult build_group(mcfftPlan p, int ndim, const int64_t* dims, int64_t batc
 // in a row (its tables stay in shared memory), and the intermediate is read
 // back while it is in L2.
 mcfftResult build_queue(mcfftPlan p) {
-  if (p->split) return MCFFT_SUCCESS;
   bool want = p->ngroups > 1;
   if (const char* e = std::getenv("MCFFT_QUEUE")) want = std::atoi(e) != 0;
   if (!want) return MCFFT_SUCCESS;
   const size_t np = p->passes.size();
   if (np > (size_t)kQueueMaxPasses) return MCFFT_SUCCESS;
   for (const auto& ps : p->passes)
-    if (!ps.tiled || ps.tp.k->split ||
-        queue_variant(ps.tp.k->L, ps.tp.k->posttw, ps.tp.k->tile_points) < 0) {
+    if (!ps.tiled || queue_variant(*ps.tp.k) < 0) {
       if (std::getenv("MCFFT_DEBUG_PLAN"))
         fprintf(stderr, "[mcfft] no batch queue: pass L=%lld not on a queue tile variant\n",
                 (long long)(ps.tiled ? ps.tp.k->L : ps.k->L));
       return MCFFT_SUCCESS;
     }
-  const int maxg = queue_max_grid(p->sms);
+  const int maxg = queue_max_grid(p->sms, p->split);
   if (maxg <= 0) return MCFFT_SUCCESS;
   Queue& q = p->q;
   q.wait_base.assign(np, -1);
@@ -691,6 +687,7 @@ mcfftResult exec_queue(mcfftPlan p, const void* in, void* out, int dir, cudaStre
   A.counters = q.counters;
   A.status = p->status;
   A.bmat = p->bsw64[dir];
+  A.bmat_lo = p->bsw64_lo[dir];
   A.npass = (int)p->passes.size();
   auto base = [&](int b) -> char* {
     return b == kUserIn ? (char*)const_cast<void*>(in) : b == kUserOut ? (char*)out : (char*)p->scratch;
@@ -698,7 +695,9 @@ mcfftResult exec_queue(mcfftPlan p, const void* in, void* out, int dir, cudaStre
   for (size_t i = 0; i < p->passes.size(); ++i) {
     const Pass& ps = p->passes[i];
     QPass& Q = A.pass[i];
-    if (!fill_qpass(ps.tp, dir, base(ps.in_buf) + ps.in_off * 4, base(ps.out_buf) + ps.out_off * 4, &Q))
+    const int ib = ps.in_f16 ? 4 : 8, ob = ps.out_f16 ? 4 : 8;
+    if (!fill_qpass(ps.tp, dir, base(ps.in_buf) + ps.in_off * ib, base(ps.out_buf) + ps.out_off * ob,
+                    &Q))
       return MCFFT_CUDA_ERROR;
     Q.wait_base = q.wait_base[i];
     Q.wait_count = ps.wait_count;
@@ -709,7 +708,7 @@ mcfftResult exec_queue(mcfftPlan p, const void* in, void* out, int dir, cudaStre
   }
   cudaError_t e = q.ncounters ? cudaMemsetAsync(q.counters, 0, q.ncounters * sizeof(int), st)
                               : cudaSuccess;
-  if (e == cudaSuccess) e = launch_queue(A, q.grid, st);
+  if (e == cudaSuccess) e = launch_queue(A, q.grid, p->split, st);
   if (e == cudaSuccess && std::getenv("MCFFT_DEBUG_SYNC")) {
     e = cudaStreamSynchronize(st);
     fprintf(stderr, "[mcfft] queue: %d passes, %lld items, grid %d: %s\n", A.npass,

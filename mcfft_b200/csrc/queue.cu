@@ -10,11 +10,16 @@
 
 namespace mcfft {
 
-int queue_variant(int L, bool posttw, int tile_points) {
+int queue_variant(const TileKernel& k) {
+  const int L = k.L;
   if (L < 32 || L > 4096 || (L & (L - 1))) return -1;
-  if (tile_points != 16384 && tile_points != 8192) return -1;
-  if (L * 4 > tile_points) return -1;
-  return queue::variant_of(L, posttw, tile_points);
+  if (k.split) {
+    if (k.tile_points != 8192 || L > 2048) return -1;
+    return queue::variant_of(L, k.posttw, k.in16);
+  }
+  if (k.tile_points != 16384 && k.tile_points != 8192) return -1;
+  if (L * 4 > k.tile_points) return -1;
+  return queue::variant_of(L, k.posttw, k.tile_points == 8192);
 }
 
 bool fill_qpass(const TilePass& tp, int dir, const void* in, void* out, QPass* q) {
@@ -43,7 +48,7 @@ bool fill_qpass(const TilePass& tp, int dir, const void* in, void* out, QPass* q
   q->out_ndims = a.out_ndims;
   q->col_blocks = a.col_blocks;
   q->in_tile_bytes = a.in_tile_bytes;
-  q->variant = queue_variant(tp.k->L, tp.k->posttw, tp.k->tile_points);
+  q->variant = queue_variant(*tp.k);
   q->wait_base = -1;
   q->sig_base = -1;
   q->sig_mul = 1;
@@ -51,15 +56,16 @@ bool fill_qpass(const TilePass& tp, int dir, const void* in, void* out, QPass* q
   return q->variant >= 0;
 }
 
-cudaError_t launch_queue(const QArgs& a, int grid, cudaStream_t st) {
-  const void* fn = reinterpret_cast<const void*>(&fft_queue_f16);
-  static std::once_flag once;
-  static cudaError_t attr = cudaSuccess;
-  std::call_once(once, [&] {
-    attr = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                QueueSmem::SMEM_BYTES);
-  });
-  if (attr != cudaSuccess) return attr;
+const void* queue_fn_split();  // queue_split.cu
+
+namespace {
+const void* queue_fn(bool split) {
+  return split ? queue_fn_split() : reinterpret_cast<const void*>(&fft_queue<false>);
+}
+}  // namespace
+
+cudaError_t launch_queue(const QArgs& a, int grid, bool split, cudaStream_t st) {
+  const void* fn = queue_fn(split);
   void* args[] = {const_cast<QArgs*>(&a)};
   // Cooperative: every CTA is resident, so a tile waiting for another
   // CTA's output never waits for a CTA that has not started.
@@ -67,9 +73,9 @@ cudaError_t launch_queue(const QArgs& a, int grid, cudaStream_t st) {
                                      (size_t)QueueSmem::SMEM_BYTES, st);
 }
 
-int queue_max_grid(int sms) {
+int queue_max_grid(int sms, bool split) {
   int occ = 0;
-  const void* fn = reinterpret_cast<const void*>(&fft_queue_f16);
+  const void* fn = queue_fn(split);
   if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            QueueSmem::SMEM_BYTES) != cudaSuccess ||
       cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, 17 * 32, QueueSmem::SMEM_BYTES) !=

@@ -7,13 +7,15 @@
 
 namespace mcfft {
 
-// Variant index of a pass in the batch kernel, or -1 if it has none.
-int queue_variant(int L, bool posttw, int tile_points);
+// Variant index of a tile pass in the batch kernel, or -1 if it has none.
+int queue_variant(const TileKernel& k);
 // Queue entry of a tile pass for one exec: tensor maps over in/out, tables
 // for direction `dir`; dependencies unset.  False if encoding fails.
 bool fill_qpass(const TilePass& tp, int dir, const void* in, void* out, QPass* q);
-cudaError_t launch_queue(const QArgs& a, int grid, cudaStream_t st);
-// CTAs of the batch kernel that can be resident at once (0 on error).
-int queue_max_grid(int sms);
+// Cooperative launch (queue_max_grid has configured the kernel).
+cudaError_t launch_queue(const QArgs& a, int grid, bool split, cudaStream_t st);
+// CTAs of the batch kernel that can be resident at once (0 on error); also
+// sets the kernel's shared-memory limit.
+int queue_max_grid(int sms, bool split);
 
 }  // namespace mcfft

@@ -81,9 +81,22 @@ def test_uneven_batch_plain_one_launch(gap):
         assert np.isnan(y[int(np.prod(SHAPES[0][0])) * SHAPES[0][1]])
 
 
-def test_uneven_batch_split():
+@pytest.mark.parametrize("flags", [mc.FLAG_INPUT_F16, mc.FLAG_NONE])
+def test_uneven_batch_split_one_launch(flags):
     descs, total = _layout(SHAPES, 0)
-    xr, y, _ = _run_batch(descs, total, mc.PREC_SPLIT, mc.FLAG_INPUT_F16)
+    xr, y, info = _run_batch(descs, total, mc.PREC_SPLIT, flags)
+    assert info.launches == 1, info.launches
+    assert _check_each(descs, xr, y, False) < SPLIT_TOL
+
+
+@pytest.mark.parametrize("shape,batch", [((1 << 20,), 2), ((4096,), 8), ((1024, 1024), 1),
+                                         ((32, 64, 256), 2)])
+def test_queue_forced_single_shape_split(shape, batch, monkeypatch):
+    monkeypatch.setenv("MCFFT_QUEUE", "1")
+    n = int(np.prod(shape))
+    descs = [(shape, batch, 0, 0)]
+    xr, y, info = _run_batch(descs, n * batch, mc.PREC_SPLIT, mc.FLAG_INPUT_F16, seed=n)
+    assert info.launches == 1
     assert _check_each(descs, xr, y, False) < SPLIT_TOL
 
 
