@@ -260,13 +260,14 @@ def run_ours(args, rank, world, local_rank):
     kern_ms = statistics.mean(per)
     achieved = bytes_alg / (kern_ms * 1e-3) / 1e9
     achieved_split = bytes_alg_split / (statistics.mean(per_split) * 1e-3) / 1e9
-    traffic = None
+    traffic = traffic_split = None
     tpath = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tpath):
         try:
-            traffic = json.load(open(tpath)).get(args.config, {}).get("plain")
+            tj = json.load(open(tpath)).get(args.config, {})
+            traffic, traffic_split = tj.get("plain"), tj.get("split")
         except Exception:
-            traffic = None
+            traffic = traffic_split = None
 
     result = None
     if rank == 0:
@@ -298,6 +299,7 @@ def run_ours(args, rank, world, local_rank):
                       "ratio_vs_plain": round(value_split / value, 4),
                       "roofline_frac": round(achieved_split / peak, 4),
                       "algorithmic_bytes_per_exec": bytes_alg_split,
+                      "traffic": traffic_split,
                       "form": "FP16 input split hi+lo, FP32 output"},
             "e2e": {"value": round(value_e2e, 2), "unit": "GFLOP/s",
                     "h2d_bytes_per_step": int(elems * 4), "d2h_bytes_per_step": int(elems * 4),
