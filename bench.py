@@ -22,6 +22,7 @@ import json
 import os
 import statistics
 import subprocess
+import threading
 import sys
 import time
 
@@ -55,52 +56,101 @@ def read_peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clock/throttle sampling during the timed region."""
+    """SM clock and clock-event (throttle) reasons sampled during the timed
+    region: NVML polled from a thread every ~0.2 ms (the timed regions last
+    milliseconds), nvidia-smi at 100 ms as a fallback.  Reads only."""
 
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    HW_SLOWDOWN, SW_POWER_CAP, SW_THERMAL, HW_THERMAL = 0x8, 0x4, 0x20, 0x40
 
-    def __init__(self, index: int):
-        self.index = index
+    def __init__(self, local_rank: int):
+        self.local_rank = local_rank
+        self.samples = []
+        self.reasons = set()
+        self.max_mhz = None
+        self.thread = None
         self.proc = None
+        self.stop_flag = False
+
+    def _nvml_handle(self):
+        import pynvml
+        import torch
+        pynvml.nvmlInit()
+        p = torch.cuda.get_device_properties(self.local_rank)
+        try:
+            bus = "%08X:%02X:%02X.0" % (p.pci_domain_id, p.pci_bus_id, p.pci_device_id)
+            return pynvml, pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+        except Exception:
+            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.local_rank)
 
     def start(self):
         try:
+            nv, h = self._nvml_handle()
+            self.max_mhz = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+            reasons_fn = (getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None)
+                          or nv.nvmlDeviceGetCurrentClocksThrottleReasons)
+
+            def poll():
+                while not self.stop_flag:
+                    try:
+                        self.samples.append(float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)))
+                        r = reasons_fn(h)
+                    except Exception:
+                        break
+                    for bit, nm in ((self.HW_SLOWDOWN, "hw_slowdown"),
+                                    (self.HW_THERMAL, "hw_thermal_slowdown"),
+                                    (self.SW_THERMAL, "sw_thermal_slowdown"),
+                                    (self.SW_POWER_CAP, "sw_power_cap")):
+                        if r & bit:
+                            self.reasons.add(nm)
+                    time.sleep(0.0002)
+
+            self.thread = threading.Thread(target=poll, daemon=True)
+            self.thread.start()
+            while not self.samples and self.thread.is_alive():
+                time.sleep(0.0005)  # first sample before the timed region
+            return
+        except Exception:
+            self.thread = None
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
             self.proc = subprocess.Popen(
-                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                ["nvidia-smi", "-i", str(self.local_rank), f"--query-gpu={q}",
                  "--format=csv,noheader,nounits", "-lms", "100"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except Exception:
             self.proc = None
 
     def stop(self):
-        if self.proc is None:
-            return None
-        self.proc.terminate()
-        try:
-            out, _ = self.proc.communicate(timeout=5)
-        except Exception:
-            self.proc.kill()
-            return None
-        sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in out.strip().splitlines():
-            f = [x.strip() for x in line.split(",")]
-            if len(f) < 9:
-                continue
+        if self.thread is not None:
+            self.stop_flag = True
+            self.thread.join(timeout=5)
+        elif self.proc is not None:
+            self.proc.terminate()
             try:
-                sm.append(float(f[1]))
-                mx = float(f[2])
-            except ValueError:
-                continue
-            for nm, v in zip(names, f[5:9]):
-                if v.lower() == "active":
-                    reasons.add(nm)
-        if not sm:
+                out, _ = self.proc.communicate(timeout=5)
+            except Exception:
+                self.proc.kill()
+                return None
+            names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+            for line in out.strip().splitlines():
+                f = [x.strip() for x in line.split(",")]
+                if len(f) < 9:
+                    continue
+                try:
+                    self.samples.append(float(f[1]))
+                    self.max_mhz = float(f[2])
+                except ValueError:
+                    continue
+                for nm, v in zip(names, f[5:9]):
+                    if v.lower() == "active":
+                        self.reasons.add(nm)
+        if not self.samples:
             return None
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+        return {"sm_mhz": statistics.median(self.samples), "sm_max_mhz": self.max_mhz,
+                "reasons": sorted(self.reasons), "samples": len(self.samples),
+                "source": "nvml" if self.thread is not None else "nvidia-smi"}
 
 
 def make_input(dims, batch, seed):
