@@ -218,7 +218,7 @@ __device__ __forceinline__ int64_t run_variant_split(const QArgs& a, uint32_t pi
 template <bool SPLIT>
 __global__ void __maxnreg__(96) fft_queue(const __grid_constant__ QArgs a) {
   constexpr int NCW = 16, NCT = NCW * 32, NMTMAX = 8;
-  constexpr int TMEM_COLS = SPLIT ? 128 : 256;
+  constexpr int TMEM_COLS = 256;  // plain: 8 M-tiles x 32; split: 4 M-tiles x 64
   using Q = QueueSmem;
   extern __shared__ uint8_t smem[];
   const uint32_t base_u = sm100::smem_u32(smem);

@@ -126,7 +126,10 @@ struct SplitTile {
   static constexpr int NIT_E = S::NMT * 4 / NCW;
   static constexpr int NMT = S::NMT;
   static constexpr int NST = S::NST;
-  static constexpr int TMEM_COLS = S::TMEM_COLS;
+  // Each M-tile accumulates 64 columns: [0, 32) A_hi B_hi + A_lo B_hi,
+  // [32, 64) A_hi B_lo (one N = 64 MMA reads A_hi once for both B parts).
+  static constexpr int TMEM_COLS = 2 * S::TMEM_COLS;
+  static_assert(TMEM_COLS <= 512, "tensor memory");
   static_assert(S::NMT * 4 % NCW == 0, "row blocks per warp");
   static_assert(NMT <= 16, "per-M-tile barriers");
   static_assert(NIT_P * NLD <= 8, "prologue registers");
@@ -172,6 +175,7 @@ struct SplitTile {
                                              const uint32_t (&eent)[NST][NIT_E]) {
     const int warp = ctid >> 5, lane = ctid & 31, sp = warp & 3;
     constexpr uint32_t IDESC = sm100::idesc_f16_f32(128, 32);
+    constexpr uint32_t IDESC64 = sm100::idesc_f16_f32(128, 64);
     const float tsgn = a.inverse ? 1.f : -1.f;
     const uint32_t sb = b ? x.t.sS1 : x.t.sS0;
     const uint32_t bb = b ? x.t.bS1 : x.t.bS0;
@@ -295,16 +299,15 @@ struct SplitTile {
 #pragma unroll
         for (int j = 0; j < NIT_E; ++j) {
           const uint32_t m = (warp >> 2) + j * (NCW / 4);
-          const uint32_t d = x.t.tmem + 32u * m;
+          const uint32_t d = x.t.tmem + 64u * m;
 #pragma unroll
           for (int ks = 0; ks < 2; ++ks) {
             const uint64_t ah = tile::sdesc_sw64(xs + m * 8192u + ks * 32u);
             const uint64_t al = tile::sdesc_sw64(xs + T::HALF + m * 8192u + ks * 32u);
-            const uint64_t bh = tile::sdesc_sw64(x.t.sB + ks * 32u);
-            const uint64_t bl = tile::sdesc_sw64(x.sBl + ks * 32u);
-            sm100::umma_f16(d, ah, bh, IDESC, ks);
-            sm100::umma_f16(d, al, bh, IDESC, 1);
-            sm100::umma_f16(d, ah, bl, IDESC, 1);
+            // B_hi rows then B_lo rows (contiguous): N = 64 over both
+            const uint64_t bhl = tile::sdesc_sw64(x.t.sB + ks * 32u);
+            sm100::umma_f16(d, ah, bhl, IDESC64, ks);
+            sm100::umma_f16(d, al, bhl, IDESC, 1);
           }
           sm100::umma_commit(&x.t.mmab[m]);
         }
@@ -328,7 +331,26 @@ struct SplitTile {
         if (!sm100::mbar_wait_bounded(&x.t.mmab[m], (mphase >> m) & 1u, kWaitLimit)) *x.t.abort_flag = 1;
         sm100::tc_fence_after();
         uint32_t d[32];
-        sm100::tmem_ld32(x.t.tmem + ((uint32_t)(32 * sp) << 16) + 32u * m, d);
+        {
+          // D = columns [0, 32) + columns [32, 64) of this M-tile
+          const uint32_t ta = x.t.tmem + ((uint32_t)(32 * sp) << 16) + 64u * m;
+          sm100::tmem_ld32(ta, d);
+#pragma unroll
+          for (int hh = 0; hh < 2; ++hh) {
+            uint32_t e2[16];
+            sm100::tmem_ld16(ta + 32u + 16u * hh, e2);
+            sm100::tmem_wait_ld();
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+              float u0, u1;
+              f2u(add2(f2p(__uint_as_float(d[16 * hh + 2 * q]), __uint_as_float(d[16 * hh + 2 * q + 1])),
+                       f2p(__uint_as_float(e2[2 * q]), __uint_as_float(e2[2 * q + 1]))),
+                  u0, u1);
+              d[16 * hh + 2 * q] = __float_as_uint(u0);
+              d[16 * hh + 2 * q + 1] = __float_as_uint(u1);
+            }
+          }
+        }
         if (!last) {
           const uint32_t trow = x.t.sTws + (row0 + aux) * 128u;
           const uint32_t fold = tw_fold(aux);
@@ -453,7 +475,7 @@ __global__ void __maxnreg__(96) fft_tile_split(const __grid_constant__ TileArgs 
       sm100::fence_mbar_init();
     }
     __syncwarp();
-    sm100::tmem_alloc(tmem_slot, S::TMEM_COLS);
+    sm100::tmem_alloc(tmem_slot, TL::TMEM_COLS);
     sm100::tmem_relinquish();
   } else {
     for (int i = tid; i < 128; i += NCT) {
@@ -531,7 +553,7 @@ __global__ void __maxnreg__(96) fft_tile_split(const __grid_constant__ TileArgs 
   }
   __syncthreads();
   if (tid == 0 && *abort_flag && a.status) atomicExch(a.status, kStatusTimeout);
-  if (producer) sm100::tmem_dealloc(tmem_base, S::TMEM_COLS);
+  if (producer) sm100::tmem_dealloc(tmem_base, TL::TMEM_COLS);
 }
 
 }  // namespace mcfft

@@ -17,7 +17,8 @@ TileKernel make_split() {
   using T = TileSplit<L, R, C, PT, NCW, IN16>;
   using S = TileShape<L, R, C, NCW>;
   return TileKernel{reinterpret_cast<const void*>(&fft_tile_split<L, R, C, PT, NCW, IN16>),
-                    L, R, C, PT, true, S::NT, T::SMEM_BYTES, S::TMEM_COLS, TP, IN16};
+                    L, R, C, PT, true, S::NT, T::SMEM_BYTES,
+                    SplitTile<L, R, C, PT, NCW, IN16>::TMEM_COLS, TP, IN16};
 }
 
 #define MCFFT_SPLIT_VARIANTS(PT, IN16)                                                  \
