@@ -44,6 +44,17 @@ constexpr int kVersion = 100;  // 0.1.0
 
 enum Buf { kUserIn = 0, kUserOut = 1, kScratch = 2 };
 
+struct PassSpec {
+  int64_t L;
+  bool colfast, posttw;
+  int64_t in_sp, in_sc, in_so, out_sp, out_sc, out_so;
+  int64_t ncols, nouter;
+  int in_buf, out_buf;
+  int64_t postN;
+  int in_f16, out_f16;
+  int64_t in_off, out_off;
+};
+
 struct Pass {
   bool tiled = false;  // TMA-fed kernel (tile_pass) instead of the direct one
   TilePass tp;
@@ -63,6 +74,7 @@ struct Pass {
   // ((t + 1) sig_mul - 1) / sig_div]; consumer side: tile (cb, outer) needs
   // key `outer` complete, i.e. wait_count producer tiles; `keys` = nouter.
   int grp = -1, level = 0;
+  PassSpec spec{};  // what the pass computes (kept for plan-time retuning)
   int64_t sig_mul = 1, sig_div = 1;
   int wait_count = 0;
   int64_t keys = 0;
@@ -163,16 +175,6 @@ int64_t tile_points_env() {
   return s ? std::atoll(s) : 0;
 }
 
-struct PassSpec {
-  int64_t L;
-  bool colfast, posttw;
-  int64_t in_sp, in_sc, in_so, out_sp, out_sc, out_so;
-  int64_t ncols, nouter;
-  int in_buf, out_buf;
-  int64_t postN;
-  int in_f16, out_f16;
-  int64_t in_off, out_off;
-};
 
 // Tables shared by both kernel families: stage twiddles [R'][k] (1/16 per
 // stage; skipped when tw is null) and radix-R twiddles [v][k] (1/R), for
@@ -242,7 +244,7 @@ mcfftResult make_stage_rows(mcfftPlan p, int L, int R, double scale, const float
 
 // Builds a pass on the TMA-fed kernel.  Returns MCFFT_UNSUPPORTED_SIZE when
 // the shape is outside what that kernel handles (the caller falls back).
-mcfftResult add_tile_pass(mcfftPlan p, const PassSpec& s) {
+mcfftResult add_tile_pass(mcfftPlan p, const PassSpec& s, int only_tile_points = 0) {
   if (std::getenv("MCFFT_NO_TILE")) return MCFFT_UNSUPPORTED_SIZE;
   layout::Kind ik, ok;
   if (s.in_sp == 1) ik = layout::ROW;
@@ -257,8 +259,8 @@ mcfftResult add_tile_pass(mcfftPlan p, const PassSpec& s) {
   // large per point).
   int first = 16384;
   if (const char* e = std::getenv("MCFFT_TILE_POINTS")) first = std::atoi(e);
-  const int order[2] = {p->split ? 8192 : first,
-                        p->split ? 8192 : (first == 16384 ? 8192 : 16384)};
+  int order[2] = {p->split ? 8192 : first, p->split ? 8192 : (first == 16384 ? 8192 : 16384)};
+  if (only_tile_points) order[0] = order[1] = only_tile_points;
   const int in_elem = s.in_f16 ? 4 : 8, out_elem = s.out_f16 ? 4 : 8;
   Pass ps;
   ps.tiled = true;
@@ -341,7 +343,77 @@ mcfftResult add_tile_pass(mcfftPlan p, const PassSpec& s) {
   ps.in_buf = s.in_buf; ps.out_buf = s.out_buf;
   ps.in_f16 = s.in_f16; ps.out_f16 = s.out_f16;
   ps.in_off = s.in_off; ps.out_off = s.out_off;
+  ps.spec = s;
   p->passes.push_back(ps);
+  return MCFFT_SUCCESS;
+}
+
+// Median CUDA-event time (ms) of one tile pass on the given buffers.
+float time_tile_pass(const TilePass& tp, void* a, void* b, cudaStream_t st) {
+  cudaEvent_t e0, e1;
+  if (cudaEventCreate(&e0) != cudaSuccess) return -1.f;
+  if (cudaEventCreate(&e1) != cudaSuccess) {
+    cudaEventDestroy(e0);
+    return -1.f;
+  }
+  float t[5] = {0};
+  bool ok = launch_tile_pass(tp, a, b, 0, st) == cudaSuccess &&
+            launch_tile_pass(tp, a, b, 0, st) == cudaSuccess;
+  for (int r = 0; r < 5 && ok; ++r) {
+    ok = cudaEventRecord(e0, st) == cudaSuccess && launch_tile_pass(tp, a, b, 0, st) == cudaSuccess &&
+         cudaEventRecord(e1, st) == cudaSuccess && cudaEventSynchronize(e1) == cudaSuccess &&
+         cudaEventElapsedTime(&t[r], e0, e1) == cudaSuccess;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (!ok) {
+    cudaGetLastError();
+    return -1.f;
+  }
+  std::sort(t, t + 5);
+  return t[2];
+}
+
+// Plan-time tuning of the tile shape of the plain-form passes [first, end)
+// of one transform group (`points` complex elements): each pass is timed
+// with 16K- and 8K-point tiles on scratch buffers and keeps the faster
+// (by more than 3 %).  MCFFT_AUTOTUNE=0 keeps the default shapes.
+mcfftResult autotune_group(mcfftPlan p, size_t first, int64_t points) {
+  if (p->split) return MCFFT_SUCCESS;
+  if (const char* e = std::getenv("MCFFT_AUTOTUNE"))
+    if (std::atoi(e) == 0) return MCFFT_SUCCESS;
+  bool any = false;
+  for (size_t i = first; i < p->passes.size(); ++i) any |= p->passes[i].tiled;
+  if (!any) return MCFFT_SUCCESS;
+  void *a = nullptr, *b = nullptr;
+  const size_t bytes = (size_t)points * 8;
+  if (cudaMalloc(&a, bytes) != cudaSuccess || cudaMalloc(&b, bytes) != cudaSuccess ||
+      cudaMemset(a, 0, bytes) != cudaSuccess || cudaMemset(b, 0, bytes) != cudaSuccess) {
+    cudaGetLastError();
+    if (a) cudaFree(a);
+    if (b) cudaFree(b);
+    return MCFFT_SUCCESS;  // no room to tune: keep the default shapes
+  }
+  const size_t end = p->passes.size();
+  for (size_t i = first; i < end; ++i) {
+    if (!p->passes[i].tiled) continue;
+    const int alt = p->passes[i].tp.k->tile_points == 16384 ? 8192 : 16384;
+    if (add_tile_pass(p, p->passes[i].spec, alt) != MCFFT_SUCCESS) continue;
+    Pass cand = p->passes.back();
+    p->passes.pop_back();
+    const float t0 = time_tile_pass(p->passes[i].tp, a, b, 0);
+    const float t1 = time_tile_pass(cand.tp, a, b, 0);
+    if (std::getenv("MCFFT_DEBUG_PLAN"))
+      fprintf(stderr, "[mcfft] tune pass L=%d: %d-point tiles %.4f ms, %d-point tiles %.4f ms\n",
+              p->passes[i].tp.k->L, p->passes[i].tp.k->tile_points, t0, alt, t1);
+    if (t0 > 0.f && t1 > 0.f && t1 < 0.97f * t0) {
+      cand.grp = p->passes[i].grp;
+      cand.level = p->passes[i].level;
+      p->passes[i] = cand;
+    }
+  }
+  cudaFree(a);
+  cudaFree(b);
   return MCFFT_SUCCESS;
 }
 
@@ -591,6 +663,9 @@ mcfftResult build_group(mcfftPlan p, int ndim, const int64_t* dims, int64_t batc
                         int64_t in_off, int64_t out_off, int* scale_log2) {
   const size_t first = p->passes.size();
   mcfftResult r = build_group_passes(p, ndim, dims, batch, in_off, out_off, scale_log2);
+  int64_t points = batch;
+  for (int d = 0; d < ndim; ++d) points *= dims[d];
+  if (!r) r = autotune_group(p, first, points);
   if (!r) link_group(p, first, ndim, dims, batch);
   return r;
 }
