@@ -231,6 +231,23 @@ def bench_uneven(args, torch, mc, stream, barrier, peak):
     return out
 
 
+def max_over_ranks(values, dist, device):
+    """Each value's maximum over all ranks (a timing of the whole job is
+    its slowest rank's); identity without a process group."""
+    if dist is None:
+        return [float(v) for v in values]
+    import torch
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(v) for v in t.tolist()]
+
+
+def job_rate(work_per_rank, world, ms):
+    """Whole-job throughput of N replicas: all ranks' work over the slowest
+    rank's time (work units per second)."""
+    return world * work_per_rank / (ms * 1e-3)
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
 
@@ -290,19 +307,15 @@ def run_ours(args, rank, world, local_rank):
     plan.check_status()
 
     def gmax(v):
-        if dist is None:
-            return v
-        t = torch.tensor([v], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return max_over_ranks([v], dist, dev)[0]
 
     ms = gmax(ms)
     ms_split = gmax(ms_split)
     ms_e2e = gmax(ms_e2e)
     fl = flops_5nlogn(dims, batch)
-    value = world * fl / (ms * 1e-3) / 1e9
-    value_split = world * fl / (ms_split * 1e-3) / 1e9
-    value_e2e = world * fl / (ms_e2e * 1e-3) / 1e9
+    value = job_rate(fl, world, ms) / 1e9
+    value_split = job_rate(fl, world, ms_split) / 1e9
+    value_e2e = job_rate(fl, world, ms_e2e) / 1e9
 
     peak, peak_kind = read_peaks()
     bytes_alg = info.in_bytes + info.out_bytes
