@@ -68,6 +68,24 @@ __device__ __forceinline__ float2 lds64w(uint32_t a) {
   return v;
 }
 
+// hi at window-relative address a, lo HALF bytes further (the low operand
+// lies HALF bytes after the high one in every operand buffer): one address
+// computation for both stores.
+template <int HALF>
+__device__ __forceinline__ void sts32_hl(uint32_t a, uint32_t hi, uint32_t lo) {
+  asm volatile("st.shared.b32 [%0+1024], %1;" ::"r"(a), "r"(hi) : "memory");
+  asm volatile("st.shared.b32 [%0+%2], %1;" ::"r"(a), "r"(lo), "n"(1024 + HALF) : "memory");
+}
+template <int HALF>
+__device__ __forceinline__ void sts128_hl(uint32_t a, uint4 hi, uint4 lo) {
+  asm volatile("st.shared.v4.b32 [%0+1024], {%1,%2,%3,%4};" ::"r"(a), "r"(hi.x), "r"(hi.y),
+               "r"(hi.z), "r"(hi.w)
+               : "memory");
+  asm volatile("st.shared.v4.b32 [%0+%5], {%1,%2,%3,%4};" ::"r"(a), "r"(lo.x), "r"(lo.y),
+               "r"(lo.z), "r"(lo.w), "n"(1024 + HALF)
+               : "memory");
+}
+
 // Splits the FP32 pairs (re_0, re_1), (im_0, im_1) of two points into
 // packed-FP16 hi and lo words per point.
 __device__ __forceinline__ void split_pair(uint64_t yr, uint64_t yi, uint32_t& hi0, uint32_t& hi1,
@@ -222,7 +240,6 @@ struct SplitTile {
 
     // ---------------------------------------------------------- prologue
     const uint32_t x0 = INPLACE_PROLOGUE ? bb : x.t.bA;  // stage-0 operand (hi; lo at + HALF)
-    const uint32_t x0l = x0 + T::HALF;
     // The maximum pass already holds every unit's loads in q; staging is
     // rewritten in place only after all consumers are past the barrier
     // above, which they are.
@@ -242,8 +259,8 @@ struct SplitTile {
             const float2 x = load_point<IN16>(q[j][n], jj);
             split2(make_float2(x.x * sc, x.y * sc), hi[n], lo[n]);
           }
-          sts128w(xo(st, a.sofs[sv], x0), make_uint4(hi[0], hi[1], hi[2], hi[3]));
-          sts128w(xo(st, a.sofs[sv], x0l), make_uint4(lo[0], lo[1], lo[2], lo[3]));
+          sts128_hl<T::HALF>(xo(st, a.sofs[sv], x0), make_uint4(hi[0], hi[1], hi[2], hi[3]),
+                             make_uint4(lo[0], lo[1], lo[2], lo[3]));
         }
       } else {
         const uint32_t trow = ient[j].y & 0x7FFFFFFFu;
@@ -260,8 +277,7 @@ struct SplitTile {
           for (int k = 0; k < R; ++k) {
             uint32_t hi, lo;
             split2(cmulf(x[k], tw_of(k)), hi, lo);
-            sts32w(xo(st, a.sofs[sv * R + k], x0), hi);
-            sts32w(xo(st, a.sofs[sv * R + k], x0l), lo);
+            sts32_hl<T::HALF>(xo(st, a.sofs[sv * R + k], x0), hi, lo);
           }
         };
         if (colitem) {
@@ -294,7 +310,6 @@ struct SplitTile {
     for (int s = 0; s < S::NST; ++s) {
       const uint32_t xs = ((S::NST - s) & 1) ? x.t.sA : sb;   // this stage's operand (hi)
       const uint32_t xn = ((S::NST - s) & 1) ? bb : x.t.bA;   // next stage's operand (window-relative)
-      const uint32_t xnl = xn + T::HALF;
       if (sp == 0 && lane == 0) {
 #pragma unroll
         for (int j = 0; j < NIT_E; ++j) {
@@ -370,10 +385,8 @@ struct SplitTile {
                     f2p(w[pp].x, w[pp].y), f2p(w[pp].z, w[pp].w), yr, yi);
               uint32_t h0, h1, l0, l1;
               split_pair(yr, yi, h0, h1, l0, l1);
-              sts32w(xo(dst, a.kofs[s][2 * p], xn), h0);
-              sts32w(xo(dst, a.kofs[s][2 * p], xnl), l0);
-              sts32w(xo(dst, a.kofs[s][2 * p + 1], xn), h1);
-              sts32w(xo(dst, a.kofs[s][2 * p + 1], xnl), l1);
+              sts32_hl<T::HALF>(xo(dst, a.kofs[s][2 * p], xn), h0, l0);
+              sts32_hl<T::HALF>(xo(dst, a.kofs[s][2 * p + 1], xn), h1, l1);
             }
           }
         } else if (POSTTW) {
