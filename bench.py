@@ -293,17 +293,17 @@ def run_ours(args, rank, world, local_rank):
     ms_split, per_split = time_steps(step_split, args.steps, args.warmup, torch, stream, barrier)
     splan.check_status()
 
-    # end to end through the C ABI with host buffers: H2D input, exec, D2H output
+    # End to end through the C ABI with page-locked host buffers
+    # (mcfftExecHost): every step copies the whole input in and the whole
+    # output out, pipelined over chunks of whole transforms.
     h_in = torch.from_numpy(host.view(np.uint16).copy()).pin_memory()
     h_out = torch.empty(elems * 2, dtype=torch.float16).pin_memory()
-    x_e = torch.empty(elems * 2, dtype=torch.uint16, device=dev)
 
     def step_e2e():
-        x_e.copy_(h_in, non_blocking=True)
-        plan.exec_ptr(x_e.data_ptr(), y.data_ptr(), mc.FORWARD, sptr)
-        h_out.copy_(y.view(torch.float16), non_blocking=True)
+        plan.exec_host_ptr(h_in.data_ptr(), h_out.data_ptr(), mc.FORWARD, sptr)
 
-    ms_e2e, _ = time_steps(step_e2e, max(3, args.steps // 4), 2, torch, stream, barrier)
+    ms_e2e, _ = time_steps(step_e2e, max(3, args.steps // 4), max(3, args.warmup), torch, stream,
+                           barrier)
     plan.check_status()
 
     def gmax(v):

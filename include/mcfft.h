@@ -116,6 +116,24 @@ MCFFT_API mcfftResult mcfftPlanCreateBatch(mcfftPlan* plan, const mcfftDesc* des
 MCFFT_API mcfftResult mcfftExec(mcfftPlan plan, const void* in, void* out, int direction,
                       void* stream);
 
+/* Host-buffer exec: copies `host_in` to the device, transforms it and copies
+ * the result to `host_out`, ordered on `stream` (the three steps the
+ * reference's harness runs one after another in setup / doit / finalize,
+ * source/mcfft_1d_utils.cpp; no single-call counterpart in the reference).
+ * A single-shape plan (one descriptor, zero offsets) is cut into chunks of
+ * whole transforms (about 8 MiB of input each; MCFFT_HOST_CHUNK_BYTES in
+ * the environment overrides), and the copy in of one chunk, the transform
+ * of the previous one and the copy out of the one before run at the same
+ * time; the copies overlap only for page-locked host buffers
+ * (cudaHostAlloc / cudaHostRegister).  The first call creates a plan for
+ * one chunk and two device buffers per side, held until the plan is
+ * destroyed (it synchronises the device: make it before any stream
+ * capture).  The host buffers must stay valid until `stream` passes the
+ * call and must be disjoint, or identical when input and output elements
+ * have the same size.  Layout and scale as mcfftExec. */
+MCFFT_API mcfftResult mcfftExecHost(mcfftPlan plan, const void* host_in, void* host_out,
+                                    int direction, void* stream);
+
 /* Reads back and clears the plan's device status word (synchronises the
  * plan's last stream).  MCFFT_DEVICE_TIMEOUT if a kernel gave up waiting. */
 MCFFT_API mcfftResult mcfftPlanCheckStatus(mcfftPlan plan);

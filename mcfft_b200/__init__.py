@@ -39,7 +39,7 @@ FLAG_INPUT_F16 = 1
 EXPORTS = (
     "mcfftPlanCreate1d", "mcfftPlanCreate2d", "mcfftPlanCreate3d", "mcfftPlanCreateBatch",
     "mcfftExec", "mcfftPlanCheckStatus", "mcfftPlanGetInfo", "mcfftPlanDestroy",
-    "mcfftGetErrorString", "mcfftGetVersion", "mcfftExec1dNoAlloc",
+    "mcfftGetErrorString", "mcfftGetVersion", "mcfftExec1dNoAlloc", "mcfftExecHost",
 )
 
 
@@ -81,6 +81,7 @@ def lib() -> ctypes.CDLL:
         L.mcfftPlanCreate3d.argtypes = [PP, i64, i64, i64, i64, ci, u32]
         L.mcfftPlanCreateBatch.argtypes = [PP, ctypes.POINTER(Desc), ci, ci, u32]
         L.mcfftExec.argtypes = [P, P, P, ci, P]
+        L.mcfftExecHost.argtypes = [P, P, P, ci, P]
         L.mcfftPlanCheckStatus.argtypes = [P]
         L.mcfftPlanGetInfo.argtypes = [P, ctypes.POINTER(PlanInfo)]
         L.mcfftPlanDestroy.argtypes = [P]
@@ -90,7 +91,7 @@ def lib() -> ctypes.CDLL:
         L.mcfftExec1dNoAlloc.argtypes = [P, P, i64, i64, ci, P]
         L.mcfftExec1dNoAlloc.restype = ci
         for name in ("mcfftPlanCreate1d", "mcfftPlanCreate2d", "mcfftPlanCreate3d",
-                     "mcfftPlanCreateBatch", "mcfftExec", "mcfftPlanCheckStatus",
+                     "mcfftPlanCreateBatch", "mcfftExec", "mcfftExecHost", "mcfftPlanCheckStatus",
                      "mcfftPlanGetInfo", "mcfftPlanDestroy"):
             getattr(L, name).restype = ci
         _lib = L
@@ -146,6 +147,12 @@ class Plan:
     def exec_ptr(self, in_ptr: int, out_ptr: int, direction: int = FORWARD, stream: int = 0):
         _check(lib().mcfftExec(self._h, ctypes.c_void_p(in_ptr), ctypes.c_void_p(out_ptr),
                                direction, ctypes.c_void_p(stream)), "mcfftExec")
+
+    def exec_host_ptr(self, in_ptr: int, out_ptr: int, direction: int = FORWARD, stream: int = 0):
+        """Host buffers in and out (page-locked for overlapped copies): copy
+        in, transform and copy out in pipelined chunks on `stream`."""
+        _check(lib().mcfftExecHost(self._h, ctypes.c_void_p(in_ptr), ctypes.c_void_p(out_ptr),
+                                   direction, ctypes.c_void_p(stream)), "mcfftExecHost")
 
     def exec(self, x, out=None, direction: int = FORWARD):
         """Run on torch CUDA tensors (complex32 for the FP16 forms, complex64

@@ -128,6 +128,33 @@ struct mcfftPlan_st {
   bool graphs_on = true;
   cudaStream_t capture_stream = nullptr;
   std::mutex graph_mu;
+  // Creation arguments, for the chunk plan of mcfftExecHost.
+  mcfftPrecision prec = MCFFT_PREC_FP16;
+  mcfftDesc desc0{};
+  int ndesc = 0;
+  int64_t in_extent = 0, out_extent = 0;  // bytes of the input / output buffers an exec touches
+  // mcfftExecHost state, made on its first call: the chunk schedule (runs of
+  // whole transforms) with a plan per chunk length (the plan itself when the
+  // whole batch is one chunk), a ring of device buffers per side, copy
+  // streams and the events that order the pipeline.
+  static constexpr int kHostRing = 4;
+  struct HostChunk {
+    int64_t first, count;  // transforms [first, first + count)
+    mcfftPlan plan;
+  };
+  struct HostPipe {
+    bool ready = false;
+    std::vector<std::pair<int64_t, mcfftPlan>> plans;  // chunk plans by transform count
+    std::vector<HostChunk> chunks;
+    int nbuf = 1;
+    size_t in_per = 0, out_per = 0;  // bytes per transform (one chunk: per whole buffer)
+    void* din[kHostRing] = {};
+    void* dout[kHostRing] = {};
+    cudaStream_t s_in = nullptr, s_out = nullptr;
+    cudaEvent_t start = nullptr, done = nullptr;
+    cudaEvent_t loaded[kHostRing] = {}, computed[kHostRing] = {}, stored[kHostRing] = {};
+  } host;
+  std::mutex host_mu;
 };
 
 namespace mcfft {
@@ -588,6 +615,7 @@ mcfftResult plan_begin(mcfftPlan* out, mcfftPrecision prec, unsigned flags, mcff
   cudaGetDevice(&p->device);
   cudaDeviceGetAttribute(&p->sms, cudaDevAttrMultiProcessorCount, p->device);
   p->split = prec == MCFFT_PREC_SPLIT;
+  p->prec = prec;
   if (const char* e = std::getenv("MCFFT_GRAPH")) p->graphs_on = std::atoi(e) != 0;
   if (std::getenv("MCFFT_DEBUG_SYNC")) p->graphs_on = false;
   p->flags = flags;
@@ -912,6 +940,145 @@ mcfftResult exec_launches(mcfftPlan p, const void* in, void* out, int dir, cudaS
   return MCFFT_SUCCESS;
 }
 
+// Chunk schedule of mcfftExecHost.  A single-shape plan (one descriptor,
+// no offsets) is cut into runs of whole transforms: lengths 1, 2, 4, ..
+// rising to B (the largest power of two with B transforms in at most
+// MCFFT_HOST_CHUNK_BYTES of input, default 32 MiB), runs of B, the rest in
+// powers of two, and the rising lengths again in reverse.  Short first and
+// last chunks shorten the time only one copy direction is busy (the first
+// copy in, the last copy out); long middle chunks keep the per-chunk cost
+// small.  Anything else is one chunk run by the plan itself.
+std::vector<int64_t> host_schedule(int64_t batch, int64_t big) {
+  std::vector<int64_t> head, mid;
+  int64_t rem = batch;
+  for (int64_t s = 1; s < big && rem >= 2 * s; s *= 2) {
+    head.push_back(s);
+    rem -= 2 * s;
+  }
+  for (; rem >= big; rem -= big) mid.push_back(big);
+  for (int64_t s = big; s >= 1; s /= 2)
+    if (rem >= s) {
+      mid.push_back(s);
+      rem -= s;
+    }
+  std::vector<int64_t> out = head;
+  out.insert(out.end(), mid.begin(), mid.end());
+  out.insert(out.end(), head.rbegin(), head.rend());
+  return out;
+}
+
+mcfftResult host_pipe_setup(mcfftPlan p) {
+  auto& h = p->host;
+  const mcfftDesc& d = p->desc0;
+  const bool single = p->ndesc == 1 && d.in_offset == 0 && d.out_offset == 0 && d.batch > 1;
+  size_t max_in = (size_t)p->in_extent, max_out = (size_t)p->out_extent;
+  if (single) {
+    int64_t target = int64_t(32) << 20;
+    if (const char* e = std::getenv("MCFFT_HOST_CHUNK_BYTES")) target = std::max<int64_t>(1, std::atoll(e));
+    h.in_per = (size_t)(p->info.in_bytes / d.batch);
+    h.out_per = (size_t)(p->info.out_bytes / d.batch);
+    int64_t big = 1;
+    while (2 * big <= d.batch && 2 * big * (int64_t)h.in_per <= target) big *= 2;
+    int64_t first = 0;
+    for (int64_t c : host_schedule(d.batch, big)) {
+      mcfftPlan x = nullptr;
+      if (c == d.batch) x = p;
+      for (auto& pr : h.plans)
+        if (pr.first == c) x = pr.second;
+      if (!x) {
+        mcfftDesc cd = d;
+        cd.batch = c;
+        mcfftResult r = mcfftPlanCreateBatch(&x, &cd, 1, p->prec, p->flags);
+        if (r) return r;
+        h.plans.push_back({c, x});
+      }
+      h.chunks.push_back({first, c, x});
+      first += c;
+    }
+    max_in = (size_t)big * h.in_per;
+    max_out = (size_t)big * h.out_per;
+  } else {
+    h.in_per = max_in;
+    h.out_per = max_out;
+    h.chunks.push_back({0, 1, p});
+  }
+  h.nbuf = (int)std::min<size_t>(mcfftPlan_st::kHostRing, h.chunks.size());
+  for (int b = 0; b < h.nbuf; ++b) {
+    mcfftResult r = plan_alloc(p, &h.din[b], max_in);
+    if (!r) r = plan_alloc(p, &h.dout[b], max_out);
+    if (r) return r;
+  }
+  cudaError_t e = cudaStreamCreateWithFlags(&h.s_in, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h.s_out, cudaStreamNonBlocking);
+  std::vector<cudaEvent_t*> evs = {&h.start, &h.done};
+  for (int b = 0; b < h.nbuf; ++b) {
+    evs.push_back(&h.loaded[b]);
+    evs.push_back(&h.computed[b]);
+    evs.push_back(&h.stored[b]);
+  }
+  for (cudaEvent_t* ev : evs)
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(ev, cudaEventDisableTiming);
+  if (e != cudaSuccess) return cuda_fail(e);
+  h.ready = true;
+  return MCFFT_SUCCESS;
+}
+
+void host_pipe_release(mcfftPlan p) {
+  auto& h = p->host;
+  for (auto& pr : h.plans) mcfftPlanDestroy(pr.second);
+  if (h.s_in) cudaStreamDestroy(h.s_in);
+  if (h.s_out) cudaStreamDestroy(h.s_out);
+  std::vector<cudaEvent_t> evs = {h.start, h.done};
+  for (int b = 0; b < mcfftPlan_st::kHostRing; ++b) {
+    evs.push_back(h.loaded[b]);
+    evs.push_back(h.computed[b]);
+    evs.push_back(h.stored[b]);
+  }
+  for (cudaEvent_t ev : evs)
+    if (ev) cudaEventDestroy(ev);
+  h = mcfftPlan_st::HostPipe();
+}
+
+// Chunk i, ring slot b = i % nbuf: copy in on s_in into din[b] once the
+// transform of chunk i - nbuf has read it; transform on the caller's stream
+// once chunk i is in and the copy out of chunk i - nbuf has drained dout[b];
+// copy out on s_out.  The caller's stream waits for the last copy out.
+mcfftResult exec_host(mcfftPlan p, const char* hin, char* hout, int direction, cudaStream_t st) {
+  auto& h = p->host;
+  cudaError_t e = cudaEventRecord(h.start, st);
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(h.s_in, h.start, 0);
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(h.s_out, h.start, 0);
+  const int64_t n = (int64_t)h.chunks.size();
+  for (int64_t i = 0; i < n && e == cudaSuccess; ++i) {
+    const mcfftPlan_st::HostChunk& c = h.chunks[i];
+    const int b = (int)(i % h.nbuf);
+    if (i >= h.nbuf) e = cudaStreamWaitEvent(h.s_in, h.computed[b], 0);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(h.din[b], hin + c.first * h.in_per, c.count * h.in_per,
+                          cudaMemcpyHostToDevice, h.s_in);
+    if (e == cudaSuccess) e = cudaEventRecord(h.loaded[b], h.s_in);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(st, h.loaded[b], 0);
+    if (e == cudaSuccess && i >= h.nbuf) e = cudaStreamWaitEvent(st, h.stored[b], 0);
+    if (e != cudaSuccess) break;
+    const mcfftResult r = mcfftExec(c.plan, h.din[b], h.dout[b], direction, st);
+    if (r) return r;
+    e = cudaEventRecord(h.computed[b], st);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(h.s_out, h.computed[b], 0);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(hout + c.first * h.out_per, h.dout[b], c.count * h.out_per,
+                          cudaMemcpyDeviceToHost, h.s_out);
+    if (e == cudaSuccess) e = cudaEventRecord(h.stored[b], h.s_out);
+  }
+  if (e == cudaSuccess) e = cudaEventRecord(h.done, h.s_out);
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(st, h.done, 0);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return MCFFT_CUDA_ERROR;
+  }
+  p->last_stream = st;
+  return MCFFT_SUCCESS;
+}
+
 }  // namespace
 }  // namespace mcfft
 
@@ -968,8 +1135,16 @@ mcfftResult mcfftPlanCreateBatch(mcfftPlan* plan, const mcfftDesc* descs, int co
   p->info.num_descs = count;
   p->info.elements = elements;
   const int in_b = p->split ? ((flags & MCFFT_FLAG_INPUT_F16) ? 4 : 8) : 4;
+  const int out_b = p->split ? 8 : 4;
   p->info.in_bytes = elements * in_b;
-  p->info.out_bytes = elements * (p->split ? 8 : 4);
+  p->info.out_bytes = elements * out_b;
+  p->desc0 = descs[0];
+  p->ndesc = count;
+  for (int i = 0; i < count; ++i) {
+    const int64_t len = descs[i].batch * points(descs[i]);
+    p->in_extent = std::max(p->in_extent, (descs[i].in_offset + len) * in_b);
+    p->out_extent = std::max(p->out_extent, (descs[i].out_offset + len) * out_b);
+  }
   return plan_finish(p, plan);
 }
 
@@ -1002,8 +1177,35 @@ mcfftResult mcfftExec(mcfftPlan p, const void* in, void* out, int direction, voi
   return exec_launches(p, in, out, dir, st);
 }
 
+mcfftResult mcfftExecHost(mcfftPlan p, const void* host_in, void* host_out, int direction,
+                          void* stream) {
+  if (!p) return MCFFT_INVALID_PLAN;
+  if (!host_in || !host_out) return MCFFT_INVALID_VALUE;
+  if (direction != MCFFT_FORWARD && direction != MCFFT_INVERSE) return MCFFT_INVALID_VALUE;
+  std::lock_guard<std::mutex> lk(p->host_mu);
+  if (!p->host.ready) {
+    const mcfftResult r = host_pipe_setup(p);
+    if (r) {
+      host_pipe_release(p);
+      return r;
+    }
+  }
+  // The copy out of one chunk may not overwrite input a later chunk has
+  // still to copy in: the buffers must be disjoint, or identical with
+  // chunks of equal size on both sides.
+  const char* a = static_cast<const char*>(host_in);
+  const char* b = static_cast<const char*>(host_out);
+  const bool overlap = a < b + p->out_extent && b < a + p->in_extent;
+  if (overlap && (a != b || p->host.in_per != p->host.out_per)) return MCFFT_INVALID_VALUE;
+  return exec_host(p, a, static_cast<char*>(host_out), direction, static_cast<cudaStream_t>(stream));
+}
+
 mcfftResult mcfftPlanCheckStatus(mcfftPlan p) {
   if (!p) return MCFFT_INVALID_PLAN;
+  for (auto& pr : p->host.plans) {
+    const mcfftResult r = mcfftPlanCheckStatus(pr.second);
+    if (r) return r;
+  }
   int h = 0;
   if (cudaStreamSynchronize(p->last_stream) != cudaSuccess) return MCFFT_CUDA_ERROR;
   if (cudaMemcpy(&h, p->status, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
@@ -1024,6 +1226,7 @@ mcfftResult mcfftPlanGetInfo(mcfftPlan p, mcfftPlanInfo* info) {
 
 mcfftResult mcfftPlanDestroy(mcfftPlan p) {
   if (!p) return MCFFT_INVALID_PLAN;
+  host_pipe_release(p);
   for (auto& g : p->graphs)
     if (g.exec) cudaGraphExecDestroy(g.exec);
   if (p->capture_stream) cudaStreamDestroy(p->capture_stream);
