@@ -1,4 +1,6 @@
-"""Build the native library mcfft_b200/libmcfft.so (sm_100a) in-tree.
+"""Build the native library mcfft_b200/libmcfft.so (sm_100a) in-tree, the
+reference-signature harness libraries libmcfft_{1,2,3}d.so and the timing
+drivers mcfft_perf_{1,2,3}d.
 
     python -m mcfft_b200.build            # or: python mcfft_b200/build.py
 
@@ -62,6 +64,17 @@ def _compat(dim: int) -> str:
     return out
 
 
+def _driver(dim: int) -> str:
+    """mcfft_perf_{dim}d: the command-line timing driver (csrc/perf_driver.cpp)."""
+    out = os.path.join(HERE, f"mcfft_perf_{dim}d")
+    src = os.path.join(CSRC, "perf_driver.cpp")
+    if _stale(out, [src, LIB, os.path.join(HERE, "..", "include", "mcfft.h")]):
+        subprocess.run([NVCC, *ARCH, "-O2", "-std=c++17", f"-DMCFFT_PERF_DIM={dim}", src, "-o", out,
+                        "-L" + HERE, "-lmcfft", "-Xlinker", "-rpath,$ORIGIN", "-cudart", "static"],
+                       check=True)
+    return out
+
+
 def build(verbose: bool = False) -> str:
     os.makedirs(BUILD, exist_ok=True)
     with cf.ThreadPoolExecutor(max_workers=len(SOURCES)) as ex:
@@ -69,8 +82,9 @@ def build(verbose: bool = False) -> str:
     if _stale(LIB, objs):
         subprocess.run([NVCC, *ARCH, "-shared", "-o", LIB, *objs, "-cudart", "static"],
                        check=True)
-    with cf.ThreadPoolExecutor(max_workers=3) as ex:
+    with cf.ThreadPoolExecutor(max_workers=6) as ex:
         list(ex.map(_compat, (1, 2, 3)))
+        list(ex.map(_driver, (1, 2, 3)))
     return LIB
 
 
