@@ -95,6 +95,7 @@ typedef struct {
   int64_t workspace_bytes; /* device scratch held by the plan */
   int num_descs;           /* transform groups (mcfftPlanCreateBatch) */
   int launches;            /* this library's kernel launches per exec (1: batch queue) */
+  int timed_passes;        /* passes the plan-time tuner timed (0: all from wisdom or untuned) */
 } mcfftPlanInfo;
 
 MCFFT_API mcfftResult mcfftPlanCreate1d(mcfftPlan* plan, int64_t n, int64_t batch,
@@ -121,12 +122,13 @@ MCFFT_API mcfftResult mcfftExec(mcfftPlan plan, const void* in, void* out, int d
  * reference's harness runs one after another in setup / doit / finalize,
  * source/mcfft_1d_utils.cpp; no single-call counterpart in the reference).
  * A single-shape plan (one descriptor, zero offsets) is cut into chunks of
- * whole transforms (about 8 MiB of input each; MCFFT_HOST_CHUNK_BYTES in
- * the environment overrides), and the copy in of one chunk, the transform
- * of the previous one and the copy out of the one before run at the same
- * time; the copies overlap only for page-locked host buffers
- * (cudaHostAlloc / cudaHostRegister).  The first call creates a plan for
- * one chunk and two device buffers per side, held until the plan is
+ * whole transforms (1, 2, 4, .. transforms rising to the largest power of
+ * two within 32 MiB of input -- MCFFT_HOST_CHUNK_BYTES in the environment
+ * overrides -- and falling again at the end), and the copy in of one chunk,
+ * the transforms of earlier ones and their copies out run at the same time;
+ * the copies overlap only for page-locked host buffers (cudaHostAlloc /
+ * cudaHostRegister).  The first call creates a plan per chunk length and a
+ * ring of up to four device buffers per side, held until the plan is
  * destroyed (it synchronises the device: make it before any stream
  * capture).  The host buffers must stay valid until `stream` passes the
  * call and must be disjoint, or identical when input and output elements
@@ -158,6 +160,17 @@ MCFFT_API const char* mcfftGetErrorString(mcfftResult result);
  * capture.  All calls share the arrays: calls that overlap on the GPU race. */
 MCFFT_API mcfftResult mcfftExec1dNoAlloc(const void* in, void* out, int64_t n, int64_t batch,
                                          int direction, void* stream);
+
+/* Autotuning records ("wisdom"; the reference has no tuner and no such
+ * file).  Creating a plain-form plan times each pass's two tile shapes once
+ * and records the faster per GPU model and pass; later plans in the process
+ * reuse the record instead of timing.  Export writes this process's records
+ * to a text file, Import reads such a file (adding to and replacing records;
+ * a malformed file changes nothing and returns MCFFT_INVALID_VALUE), Forget
+ * drops every record.  Records of another GPU model are kept but unused. */
+MCFFT_API mcfftResult mcfftWisdomExport(const char* path);
+MCFFT_API mcfftResult mcfftWisdomImport(const char* path);
+MCFFT_API mcfftResult mcfftWisdomForget(void);
 
 /* Library version as 10000*major + 100*minor + patch. */
 MCFFT_API int mcfftGetVersion(void);

@@ -40,6 +40,7 @@ EXPORTS = (
     "mcfftPlanCreate1d", "mcfftPlanCreate2d", "mcfftPlanCreate3d", "mcfftPlanCreateBatch",
     "mcfftExec", "mcfftPlanCheckStatus", "mcfftPlanGetInfo", "mcfftPlanDestroy",
     "mcfftGetErrorString", "mcfftGetVersion", "mcfftExec1dNoAlloc", "mcfftExecHost",
+    "mcfftWisdomExport", "mcfftWisdomImport", "mcfftWisdomForget",
 )
 
 
@@ -60,7 +61,7 @@ class PlanInfo(ctypes.Structure):
                 ("scale_log2", ctypes.c_int), ("elements", ctypes.c_int64),
                 ("in_bytes", ctypes.c_int64), ("out_bytes", ctypes.c_int64),
                 ("workspace_bytes", ctypes.c_int64), ("num_descs", ctypes.c_int),
-                ("launches", ctypes.c_int)]
+                ("launches", ctypes.c_int), ("timed_passes", ctypes.c_int)]
 
 
 _lib = None
@@ -82,6 +83,11 @@ def lib() -> ctypes.CDLL:
         L.mcfftPlanCreateBatch.argtypes = [PP, ctypes.POINTER(Desc), ci, ci, u32]
         L.mcfftExec.argtypes = [P, P, P, ci, P]
         L.mcfftExecHost.argtypes = [P, P, P, ci, P]
+        L.mcfftWisdomExport.argtypes = [ctypes.c_char_p]
+        L.mcfftWisdomImport.argtypes = [ctypes.c_char_p]
+        L.mcfftWisdomForget.argtypes = []
+        for name in ("mcfftWisdomExport", "mcfftWisdomImport", "mcfftWisdomForget"):
+            getattr(L, name).restype = ci
         L.mcfftPlanCheckStatus.argtypes = [P]
         L.mcfftPlanGetInfo.argtypes = [P, ctypes.POINTER(PlanInfo)]
         L.mcfftPlanDestroy.argtypes = [P]
@@ -193,6 +199,20 @@ def exec_1d_no_alloc(in_ptr: int, out_ptr: int, n: int, batch: int,
     device arrays inside the library; see include/mcfft.h)."""
     _check(lib().mcfftExec1dNoAlloc(ctypes.c_void_p(in_ptr), ctypes.c_void_p(out_ptr), n, batch,
                                     direction, ctypes.c_void_p(stream)), "mcfftExec1dNoAlloc")
+
+
+def wisdom_export(path: str):
+    """Write this process's autotuning records to `path`."""
+    _check(lib().mcfftWisdomExport(os.fsencode(path)), "mcfftWisdomExport")
+
+
+def wisdom_import(path: str):
+    """Read autotuning records; later plans reuse them instead of timing."""
+    _check(lib().mcfftWisdomImport(os.fsencode(path)), "mcfftWisdomImport")
+
+
+def wisdom_forget():
+    _check(lib().mcfftWisdomForget(), "mcfftWisdomForget")
 
 
 def version() -> int:

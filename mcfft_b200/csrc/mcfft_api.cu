@@ -401,17 +401,89 @@ float time_tile_pass(const TilePass& tp, void* a, void* b, cudaStream_t st) {
   return t[2];
 }
 
+// Autotuning records ("wisdom"): the tile shape the plan-time tuner chose
+// for a pass, keyed by the GPU (name and SM count) and everything the
+// choice depends on (the pass's length, layout, strides and extents).  The
+// records of this process can be written to a text file and read back by a
+// later process, whose plans then take the recorded shapes without timing.
+// File format: the line "mcfft-wisdom 1", then one record per line:
+// "<gpu name>\t<sms>\t<pass key>\t<tile points>".
+struct Wisdom {
+  std::mutex mu;
+  std::vector<std::pair<std::string, int>> recs;  // key (gpu + pass) -> tile points
+};
+Wisdom& wisdom() {
+  static Wisdom w;
+  return w;
+}
+
+std::string gpu_key(const mcfftPlan p) {
+  cudaDeviceProp prop{};
+  if (cudaGetDeviceProperties(&prop, p->device) != cudaSuccess) {
+    cudaGetLastError();
+    prop.name[0] = 0;
+  }
+  std::string name(prop.name);
+  for (char& c : name)
+    if (c == '\t' || c == '\n') c = ' ';
+  return name + "\t" + std::to_string(p->sms);
+}
+
+std::string pass_key(const PassSpec& s) {
+  char b[512];
+  std::snprintf(b, sizeof b, "L%lld c%d t%d i%lld,%lld,%lld o%lld,%lld,%lld n%lld,%lld h%d,%d N%lld",
+                (long long)s.L, (int)s.colfast, (int)s.posttw, (long long)s.in_sp, (long long)s.in_sc,
+                (long long)s.in_so, (long long)s.out_sp, (long long)s.out_sc, (long long)s.out_so,
+                (long long)s.ncols, (long long)s.nouter, s.in_f16, s.out_f16, (long long)s.postN);
+  return b;
+}
+
+int wisdom_find(const std::string& key) {
+  Wisdom& w = wisdom();
+  std::lock_guard<std::mutex> lk(w.mu);
+  for (auto& r : w.recs)
+    if (r.first == key) return r.second;
+  return 0;
+}
+
+void wisdom_put(const std::string& key, int tile_points) {
+  Wisdom& w = wisdom();
+  std::lock_guard<std::mutex> lk(w.mu);
+  for (auto& r : w.recs)
+    if (r.first == key) {
+      r.second = tile_points;
+      return;
+    }
+  w.recs.push_back({key, tile_points});
+}
+
 // Plan-time tuning of the tile shape of the plain-form passes [first, end)
-// of one transform group (`points` complex elements): each pass is timed
-// with 16K- and 8K-point tiles on scratch buffers and keeps the faster
-// (by more than 3 %).  MCFFT_AUTOTUNE=0 keeps the default shapes.
+// of one transform group (`points` complex elements): each pass takes the
+// shape recorded for it, or is timed with 16K- and 8K-point tiles on
+// scratch buffers and keeps the faster (by more than 3 %), which is then
+// recorded.  MCFFT_AUTOTUNE=0 keeps the default shapes.
 mcfftResult autotune_group(mcfftPlan p, size_t first, int64_t points) {
   if (p->split) return MCFFT_SUCCESS;
   if (const char* e = std::getenv("MCFFT_AUTOTUNE"))
     if (std::atoi(e) == 0) return MCFFT_SUCCESS;
-  bool any = false;
-  for (size_t i = first; i < p->passes.size(); ++i) any |= p->passes[i].tiled;
-  if (!any) return MCFFT_SUCCESS;
+  const std::string gk = gpu_key(p);
+  std::vector<size_t> todo;
+  for (size_t i = first; i < p->passes.size(); ++i) {
+    if (!p->passes[i].tiled) continue;
+    const int rec = wisdom_find(gk + "\t" + pass_key(p->passes[i].spec));
+    if (!rec) {
+      todo.push_back(i);
+      continue;
+    }
+    if (rec == p->passes[i].tp.k->tile_points) continue;
+    if (add_tile_pass(p, p->passes[i].spec, rec) != MCFFT_SUCCESS) continue;
+    Pass cand = p->passes.back();
+    p->passes.pop_back();
+    cand.grp = p->passes[i].grp;
+    cand.level = p->passes[i].level;
+    p->passes[i] = cand;
+  }
+  if (todo.empty()) return MCFFT_SUCCESS;
   void *a = nullptr, *b = nullptr;
   const size_t bytes = (size_t)points * 8;
   if (cudaMalloc(&a, bytes) != cudaSuccess || cudaMalloc(&b, bytes) != cudaSuccess ||
@@ -421,15 +493,14 @@ mcfftResult autotune_group(mcfftPlan p, size_t first, int64_t points) {
     if (b) cudaFree(b);
     return MCFFT_SUCCESS;  // no room to tune: keep the default shapes
   }
-  const size_t end = p->passes.size();
-  for (size_t i = first; i < end; ++i) {
-    if (!p->passes[i].tiled) continue;
+  for (size_t i : todo) {
     const int alt = p->passes[i].tp.k->tile_points == 16384 ? 8192 : 16384;
     if (add_tile_pass(p, p->passes[i].spec, alt) != MCFFT_SUCCESS) continue;
     Pass cand = p->passes.back();
     p->passes.pop_back();
     const float t0 = time_tile_pass(p->passes[i].tp, a, b, 0);
     const float t1 = time_tile_pass(cand.tp, a, b, 0);
+    ++p->info.timed_passes;
     if (std::getenv("MCFFT_DEBUG_PLAN"))
       fprintf(stderr, "[mcfft] tune pass L=%d: %d-point tiles %.4f ms, %d-point tiles %.4f ms\n",
               p->passes[i].tp.k->L, p->passes[i].tp.k->tile_points, t0, alt, t1);
@@ -438,6 +509,8 @@ mcfftResult autotune_group(mcfftPlan p, size_t first, int64_t points) {
       cand.level = p->passes[i].level;
       p->passes[i] = cand;
     }
+    if (t0 > 0.f && t1 > 0.f)
+      wisdom_put(gk + "\t" + pass_key(p->passes[i].spec), p->passes[i].tp.k->tile_points);
   }
   cudaFree(a);
   cudaFree(b);
@@ -1233,6 +1306,58 @@ mcfftResult mcfftPlanDestroy(mcfftPlan p) {
   for (void* d : p->allocs) cudaFree(d);
   delete p->q.args;
   delete p;
+  return MCFFT_SUCCESS;
+}
+
+mcfftResult mcfftWisdomExport(const char* path) {
+  if (!path) return MCFFT_INVALID_VALUE;
+  FILE* f = std::fopen(path, "w");
+  if (!f) return MCFFT_INVALID_VALUE;
+  Wisdom& w = wisdom();
+  std::lock_guard<std::mutex> lk(w.mu);
+  bool ok = std::fprintf(f, "mcfft-wisdom 1\n") > 0;
+  for (auto& r : w.recs) ok = ok && std::fprintf(f, "%s\t%d\n", r.first.c_str(), r.second) > 0;
+  ok = (std::fclose(f) == 0) && ok;
+  return ok ? MCFFT_SUCCESS : MCFFT_INVALID_VALUE;
+}
+
+mcfftResult mcfftWisdomImport(const char* path) {
+  if (!path) return MCFFT_INVALID_VALUE;
+  FILE* f = std::fopen(path, "r");
+  if (!f) return MCFFT_INVALID_VALUE;
+  std::vector<std::pair<std::string, int>> got;
+  char line[1024];
+  bool ok = std::fgets(line, sizeof line, f) && std::strcmp(line, "mcfft-wisdom 1\n") == 0;
+  while (ok && std::fgets(line, sizeof line, f)) {
+    std::string l(line);
+    if (!l.empty() && l.back() == '\n') {
+      l.pop_back();
+    } else if (!std::feof(f)) {
+      ok = false;  // a line longer than the buffer
+      break;
+    }
+    if (l.empty()) continue;
+    // four tab-separated fields; the value is a supported tile size
+    const size_t t3 = l.rfind('\t');
+    size_t tabs = 0;
+    for (char c : l) tabs += c == '\t';
+    if (tabs != 3 || t3 == std::string::npos) { ok = false; break; }
+    const std::string v = l.substr(t3 + 1);
+    char* end = nullptr;
+    const long tp = std::strtol(v.c_str(), &end, 10);
+    if (v.empty() || *end || (tp != 8192 && tp != 16384)) { ok = false; break; }
+    got.push_back({l.substr(0, t3), (int)tp});
+  }
+  std::fclose(f);
+  if (!ok) return MCFFT_INVALID_VALUE;
+  for (auto& r : got) wisdom_put(r.first, r.second);
+  return MCFFT_SUCCESS;
+}
+
+mcfftResult mcfftWisdomForget(void) {
+  Wisdom& w = wisdom();
+  std::lock_guard<std::mutex> lk(w.mu);
+  w.recs.clear();
   return MCFFT_SUCCESS;
 }
 
