@@ -357,10 +357,13 @@ __device__ __forceinline__ void small_dft_h2(__half2 (&x)[R], float sgn) {
 
 // Four-step twiddles of this thread's epilogue rows, w[j] = {W_N^(v g),
 // W_N^(NV g)} for row j (vector v of column g), computed before the MMA
-// wait so that their cost overlaps it.  N <= 2^24: FP32 sincospif of the
-// exact angle e (2 / N) (e / N is exact in FP32); larger N: the two-level
+// wait so that their cost overlaps it.  N <= 2^24: the exact angle
+// x = e (2 / N) (e / N is exact in FP32) -- FAST (plain form): x reduced to
+// [-1, 1) and the hardware sine / cosine of pi x (__sincosf, absolute error
+// below 1e-6, three orders of magnitude under the FP16 rounding of the
+// output); otherwise FP32 sincospif (split form).  Larger N: the two-level
 // table product lo[e & (2^sh - 1)] * hi[e >> sh].
-template <int C, int NV, int NIT_E, int NST, class A>
+template <int C, int NV, bool FAST, int NIT_E, int NST, class A>
 __device__ __forceinline__ void post_twiddles(const A& a, int64_t cb, int s,
                                               const uint32_t (&eent)[NST][NIT_E],
                                               float2 (&w)[NIT_E][2]) {
@@ -375,7 +378,13 @@ __device__ __forceinline__ void post_twiddles(const A& a, int64_t cb, int s,
     for (int h = 0; h < 2; ++h) {
       if (a.post_scale != 0.f) {
         float sn, cs;
-        sincospif((float)e[h] * a.post_scale, &sn, &cs);
+        if constexpr (FAST) {
+          float xr = (float)e[h] * a.post_scale;  // [0, 2)
+          xr = xr >= 1.f ? xr - 2.f : xr;
+          __sincosf(xr * 3.14159265358979f, &sn, &cs);  // pi x
+        } else {
+          sincospif((float)e[h] * a.post_scale, &sn, &cs);
+        }
         w[j][h] = make_float2(cs, sgn * sn);
       } else {
         w[j][h] = cmulf(__ldg(a.post_a + (e[h] & lmask)), __ldg(a.post_b + (e[h] >> a.post_shift)));
@@ -584,7 +593,7 @@ struct F16Tile {
     const bool last = s == S::NST - 1;
     const uint32_t row0 = stage_tw_row0<L, R>(s);
     float2 pt[NIT_E][2];
-    if constexpr (POSTTW && s == S::NST - 1) post_twiddles<C, S::NV>(a, cb, s, eent, pt);
+    if constexpr (POSTTW && s == S::NST - 1) post_twiddles<C, S::NV, true>(a, cb, s, eent, pt);
 #pragma unroll
     for (int j = 0; j < NIT_E; ++j) {
       const uint32_t m = (warp >> 2) + j * (NCW / 4);

@@ -330,7 +330,7 @@ struct SplitTile {
       const bool last = s == S::NST - 1;
       const uint32_t row0 = stage_tw_row0<L, R>(s);
       float2 pt[NIT_E][2];
-      if (POSTTW && last) post_twiddles<C, S::NV>(a, cb, s, eent, pt);
+      if (POSTTW && last) post_twiddles<C, S::NV, false>(a, cb, s, eent, pt);
 #pragma unroll
       for (int j = 0; j < NIT_E; ++j) {
         const uint32_t m = (warp >> 2) + j * (NCW / 4);
