@@ -58,7 +58,8 @@ struct alignas(64) QPass {
   int32_t wait_base;    // counters[wait_base + outer] >= wait_count before loading; -1: none
   int32_t wait_count;
   int32_t sig_base;     // after the store of tile t: +1 on counters[sig_base + k] for every
-  int32_t pad_;         //   k in [t sig_mul / sig_div, ((t + 1) sig_mul - 1) / sig_div],
+                        //   k in [t sig_mul / sig_div, ((t + 1) sig_mul - 1) / sig_div],
+  int32_t tail_pm;      // radix-R table layout (tail_layout.h)
   int64_t sig_mul, sig_div, sig_kmax;  // k <= sig_kmax; sig_base -1: none
 };
 

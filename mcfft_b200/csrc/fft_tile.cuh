@@ -33,6 +33,7 @@
 #include "fft_pass.cuh"
 #include "mcfft_internal.h"
 #include "sm100_ptx.cuh"
+#include "tail_layout.h"
 
 namespace mcfft {
 
@@ -62,6 +63,7 @@ struct alignas(64) TileArgs {
   float out_scale;         // split form: applied after the last stage (the plain form keeps its 1/16 per stage in the DFT-16 matrix)
   int inverse;
   int split_in_f16;
+  int32_t tail_pm;         // radix-R table layout (tail_layout.h): -1 natural, t >= 0 folded
   int* status;
 };
 
@@ -446,8 +448,9 @@ struct F16Tile {
       }
   }
 
-  // Radix-R twiddles (as packed-FP16 pairs {(wr, wr), (-wi, wi)}) and stage
-  // twiddle rows into shared memory; consumer threads only.
+  // Radix-R twiddles (as packed-FP16 pairs {(wr, wr), (-wi, wi)}, laid out
+  // as a.tail_pm says) and stage twiddle rows into shared memory; consumer
+  // threads only.
   template <class A>
   static __device__ __forceinline__ void tables(const A& a, uint8_t* tail, uint8_t* tws, int ctid) {
     if constexpr (R > 1) {
@@ -458,7 +461,7 @@ struct F16Tile {
         uint2 v;
         v.x = *reinterpret_cast<const uint32_t*>(&wrr);
         v.y = *reinterpret_cast<const uint32_t*>(&wni);
-        *reinterpret_cast<uint2*>(tail + 8 * i) = v;
+        *reinterpret_cast<uint2*>(tail + tail_entry(i / R, i % R, R, a.tail_pm)) = v;
       }
     }
     if constexpr (T::TW_SMEM && T::TW_ROWS > 0) {
@@ -533,10 +536,12 @@ struct F16Tile {
           }
         };
         if (colitem) {
-          // column items: the four sub-vectors share one twiddle row
+          // column items (folded table): the four sub-vectors share one
+          // twiddle row
           uint4 twc[R / 2];
 #pragma unroll
-          for (int k2 = 0; k2 < R / 2; ++k2) twc[k2] = tile::lds128(x.sTail + trow * (R * 8) + 16 * k2);
+          for (int k2 = 0; k2 < R / 2; ++k2)
+            twc[k2] = tile::lds128(x.sTail + tail_offset(trow, 2 * k2, R));
 #pragma unroll
           for (int jj = 0; jj < 4; ++jj) subvec(jj, [&](int k2) { return twc[k2]; });
         } else {

@@ -178,7 +178,8 @@ struct SplitTile {
   static __device__ __forceinline__ void tables(const A& a, uint8_t* tail, uint8_t* tws, int ctid) {
     if constexpr (R > 1) {
       for (int i = ctid; i < L; i += NCT)
-        *reinterpret_cast<float2*>(tail + 8 * i) = __ldg(a.tail_tw + i);
+        *reinterpret_cast<float2*>(tail + tail_entry(i / R, i % R, R, a.tail_pm)) =
+            __ldg(a.tail_tw + i);
     }
     if constexpr (T::TW_SMEM && T::TW_ROWS > 0) {
       for (int i = ctid; i < T::TW_ROWS * 8; i += NCT)
@@ -285,7 +286,7 @@ struct SplitTile {
           float2 wc[R];
 #pragma unroll
           for (int k = 0; k < R; ++k) {
-            const float2 w = lds64f(x.t.sTail + (trow * R + k) * 8);
+            const float2 w = lds64f(x.t.sTail + tail_offset(trow, k, R));
             wc[k] = make_float2(w.x * sc, w.y * sc);
           }
 #pragma unroll

@@ -2,6 +2,7 @@
 #include "layout.h"
 
 #include <algorithm>
+#include <cstdlib>
 #include <cstdio>
 #include <functional>
 #include <map>
@@ -98,21 +99,47 @@ double ideal_wavefronts(size_t lanes, int bytes) {
 
 uint32_t Staging::offset(uint32_t pos, uint32_t c) const {
   uint32_t raw;
-  if (kind == ROW)
+  if (kind == ROW) {
     raw = ((pos / E) * C + c) * row_bytes + (pos % E) * elem;
-  else
-    raw = ((c / E) * L + pos) * row_bytes + (c % E) * elem;
+  } else {
+    uint32_t prow = pos;
+    if (pmid >= 0) {
+      const uint32_t lo = pos & ((1u << pmid) - 1u), mid = (pos >> pmid) & 7u;
+      prow = mid | (lo << 3) | ((pos >> (pmid + 3)) << (pmid + 3));
+    }
+    raw = ((c / E) * L + prow) * row_bytes + (c % E) * elem;
+  }
   return raw ^ (((raw >> 7) & swz) << 4);
 }
 
 Staging make_staging(Kind kind, int L, int C, int elem, int64_t sp, int64_t sc, int64_t so,
-                     int64_t ncols, int64_t nouter) {
+                     int64_t ncols, int64_t nouter, int pmid) {
   Staging s;
   s.kind = kind;
   s.L = L;
   s.C = C;
   s.elem = elem;
   const int per_row = 128 / elem;
+  if (kind == COL && pmid >= 1) {
+    // Permuted point order (see Staging::pmid): all C columns in one
+    // shared-memory row; dims columns, point bits [t, t+3), [0, t), the
+    // rest, outer.  The column block is the innermost coordinate (cb * C).
+    s.pmid = pmid;
+    s.E = C;
+    s.row_bytes = C * elem;
+    s.swz = swz_for(s.row_bytes);
+    const uint64_t nlo = uint64_t(1) << pmid, nhi = (uint64_t)L >> (pmid + 3);
+    s.ndims = 5;
+    s.gdim[0] = (uint64_t)ncols;  s.box[0] = (uint32_t)C;
+    s.gdim[1] = 8;                s.box[1] = 8;                 s.gstride_bytes[1] = nlo * sp * elem;
+    s.gdim[2] = nlo;              s.box[2] = (uint32_t)nlo;     s.gstride_bytes[2] = (uint64_t)sp * elem;
+    s.gdim[3] = nhi;              s.box[3] = (uint32_t)nhi;     s.gstride_bytes[3] = 8 * nlo * sp * elem;
+    s.gdim[4] = (uint64_t)nouter; s.box[4] = 1;                 s.gstride_bytes[4] = (uint64_t)so * elem;
+    s.cmul[0] = C;
+    s.omul[4] = 1;
+    if (nouter <= 1) s.ndims = 4;
+    return s;
+  }
   if (kind == ROW) {
     s.E = std::min(L, per_row);
     s.row_bytes = s.E * elem;
@@ -309,7 +336,9 @@ double eval_prologue(const Ctx& x, const RowMap& m0, const std::vector<int>& ord
     }
     lb[it] = la[(size_t)it * nl];
     sb[it] = sa[(size_t)it * ns];
-    tw[it] = p.R == 1 ? 0 : (p.in_kind == ROW ? 4 * f[1] : (f[0] | 0x80000000u));
+    tw[it] = p.R == 1 ? 0
+             : p.in_kind == ROW ? 4 * f[1]
+                                : (tail_row(f[0], std::max(p.in.pmid, 0)) | 0x80000000u);
     if (fill) {
       for (int j = 0; j < nl; ++j) {
         uint32_t o = la[(size_t)it * nl + j] ^ lb[it];
@@ -454,7 +483,12 @@ bool build(PassLayout* pl, int L, int R, int C, Kind in_kind, Kind out_kind, int
   std::vector<std::pair<double, int>> xr, yr;
   const std::vector<int> ydef = ys[0];
   int xzero = 0, yzero = 0;
-  for (int ix = 0; ix < (nst > 1 ? (int)xs.size() : 1) && xzero < 12; ++ix) {
+  // Column input that can use a permuted staging (below) needs more
+  // choices for the bits of A row 0..2: the prologue's stores decide among
+  // the epilogue-optimal maps.
+  const bool permutable = in_kind == COL && C * in_elem <= 128 && ncols >= C;
+  const int xcap = permutable ? 64 : 12, ycap = permutable ? 8 : 24;
+  for (int ix = 0; ix < (nst > 1 ? (int)xs.size() : 1) && xzero < xcap; ++ix) {
     std::vector<RowMap> maps;
     if (!maps_for(xs[ix], ydef, &maps)) { if (nst > 2) continue; }
     double c = 0;
@@ -479,8 +513,8 @@ bool build(PassLayout* pl, int L, int R, int C, Kind in_kind, Kind out_kind, int
   std::sort(yr.begin(), yr.end());
   struct Cand { double cost; std::vector<RowMap> maps; };
   std::vector<Cand> cands;
-  for (size_t i = 0; i < std::min<size_t>(xr.size(), 12); ++i) {
-    for (size_t j = 0; j < std::min<size_t>(yr.size(), 24); ++j) {
+  for (size_t i = 0; i < std::min<size_t>(xr.size(), xcap); ++i) {
+    for (size_t j = 0; j < std::min<size_t>(yr.size(), ycap); ++j) {
       std::vector<RowMap> maps;
       if (!maps_for(xs[xr[i].second], ys[yr[j].second], &maps)) continue;
       double c = xr[i].first + yr[j].first;
@@ -493,6 +527,22 @@ bool build(PassLayout* pl, int L, int R, int C, Kind in_kind, Kind out_kind, int
   if (cands.empty()) { *err = "no linear row map"; return false; }
   std::stable_sort(cands.begin(), cands.end(),
                    [](const Cand& a, const Cand& b) { return a.cost < b.cost; });
+  if (permutable) {
+    // among equally good maps, alternate the source of stage 0's row bit 0
+    // (what the prologue's store banks depend on most)
+    std::map<int, int> seen;
+    std::vector<std::pair<std::pair<double, int>, size_t>> key;
+    for (size_t i = 0; i < cands.size(); ++i)
+      key.push_back({{cands[i].cost, seen[cands[i].maps[0].src[0]]++}, i});
+    std::stable_sort(key.begin(), key.end(), [](const auto& a, const auto& b) {
+      if (a.first.first < b.first.first - 1e-9) return true;
+      if (b.first.first < a.first.first - 1e-9) return false;
+      return a.first.second < b.first.second;
+    });
+    std::vector<Cand> re;
+    for (auto& k : key) re.push_back(cands[k.second]);
+    cands.swap(re);
+  }
 
   // Prologue item order for the best few row-map candidates: 5 lane bits
   // among the item-coordinate bits (first three = one 8-lane phase).
@@ -516,50 +566,70 @@ bool build(PassLayout* pl, int L, int R, int C, Kind in_kind, Kind out_kind, int
       off += w;
     }
   }
+  // Input staging candidates: for column input whose C columns fit one
+  // shared-memory row (and a pass at least C columns wide) first the
+  // permuted order that brings point bits [t, t+3) to the bank-selecting
+  // row bits, t = lg(L/R) - 4 -- the A stores of an item are conflict-free
+  // when the lanes differ in the stage-0 K position, point bits
+  // [lg(L/R) - 4, lg(L/R)), which the natural order leaves out of the load
+  // banks -- then, unless that layout is conflict-free, the natural order,
+  // which wins ties.
+  std::vector<int> pmids = {-1};
+  const int tstar = ilog2(L / R) - 4;
+  if (permutable && tstar >= 1 && tstar <= ilog2(L) - 3) pmids.insert(pmids.begin(), tstar);
   double total_best = 1e30;
   std::vector<int> porder_best;
   std::vector<RowMap> maps_best;
+  Staging in_best = p.in;
   const int epi_weight = 16 * nst;  // epilogue instructions per row-warp vs prologue per item-warp
-  for (size_t ci = 0; ci < std::min<size_t>(cands.size(), 4); ++ci) {
-    if (ci > 0 && cands[ci].cost > cands[0].cost + 1e-9) break;
-    double pbest = 1e30;
-    std::vector<int> porder;
-    std::vector<int> comb(nl);
-    std::function<void(int, int)> rec = [&](int start, int depth) {
-      if (pbest < 1e-9) return;
-      if (depth == nl) {
-        // which 3 of the 5 lane bits form the 8-lane phase
-        for (int m = 0; m < (1 << nl) && pbest > 1e-9; ++m) {
-          if (__builtin_popcount(m) != std::min(3, nl)) continue;
-          std::vector<int> order;
-          for (int i = 0; i < nl; ++i) if (m >> i & 1) order.push_back(comb[i]);
-          for (int i = 0; i < nl; ++i) if (!(m >> i & 1)) order.push_back(comb[i]);
-          std::set<int> u(order.begin(), order.end());
-          for (int i = 0; i < nb; ++i)
-            if (!u.count(i)) order.push_back(i);
-          bool lin = true;
-          double c = eval_prologue(x, cands[ci].maps[0], order, false, &lin);
-          if (lin && c < pbest - 1e-9) {
-            pbest = c;
-            porder = order;
+  for (int pm : pmids) {
+    if (total_best <= cands[0].cost * epi_weight / 16.0 + 1e-9) break;  // cannot do better
+    p.in = make_staging(in_kind, L, C, in_elem, in_sp, in_sc, in_so, ncols, nouter, pm);
+    for (size_t ci = 0; ci < std::min<size_t>(cands.size(), permutable ? 32 : 4); ++ci) {
+      if (ci > 0 && cands[ci].cost > cands[0].cost + 1e-9) break;
+      if (total_best <= cands[0].cost * epi_weight / 16.0 + 1e-9) break;  // found the optimum
+      double pbest = 1e30;
+      std::vector<int> porder;
+      std::vector<int> comb(nl);
+      std::function<void(int, int)> rec = [&](int start, int depth) {
+        if (pbest < 1e-9) return;
+        if (depth == nl) {
+          // which 3 of the 5 lane bits form the 8-lane phase
+          for (int m = 0; m < (1 << nl) && pbest > 1e-9; ++m) {
+            if (__builtin_popcount(m) != std::min(3, nl)) continue;
+            std::vector<int> order;
+            for (int i = 0; i < nl; ++i) if (m >> i & 1) order.push_back(comb[i]);
+            for (int i = 0; i < nl; ++i) if (!(m >> i & 1)) order.push_back(comb[i]);
+            std::set<int> u(order.begin(), order.end());
+            for (int i = 0; i < nb; ++i)
+              if (!u.count(i)) order.push_back(i);
+            bool lin = true;
+            double c = eval_prologue(x, cands[ci].maps[0], order, false, &lin);
+            if (lin && c < pbest - 1e-9) {
+              pbest = c;
+              porder = order;
+            }
           }
+          return;
         }
-        return;
+        for (size_t i = start; i < lane_pool.size(); ++i) {
+          comb[depth] = lane_pool[i];
+          rec((int)i + 1, depth + 1);
+        }
+      };
+      rec(0, 0);
+      if (porder.empty()) continue;
+      const double total = pbest + cands[ci].cost * epi_weight / 16.0;
+      if (total < total_best - 1e-9 || (pm < 0 && total <= total_best + 1e-9)) {
+        total_best = total;
+        porder_best = porder;
+        maps_best = cands[ci].maps;
+        in_best = p.in;
       }
-      for (size_t i = start; i < lane_pool.size(); ++i) {
-        comb[depth] = lane_pool[i];
-        rec((int)i + 1, depth + 1);
-      }
-    };
-    rec(0, 0);
-    if (porder.empty()) continue;
-    const double total = pbest + cands[ci].cost * epi_weight / 16.0;
-    if (total < total_best - 1e-9) {
-      total_best = total;
-      porder_best = porder;
-      maps_best = cands[ci].maps;
     }
   }
+  p.in = in_best;
+  p.tail_pm = (in_kind == COL && R > 1) ? std::max(p.in.pmid, 0) : -1;
   if (porder_best.empty()) { *err = "no linear prologue"; return false; }
   std::vector<RowMap> best_maps = maps_best;
   {

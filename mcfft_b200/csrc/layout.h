@@ -23,6 +23,8 @@
 #include <string>
 #include <vector>
 
+#include "tail_layout.h"
+
 namespace mcfft {
 namespace layout {
 
@@ -34,6 +36,10 @@ struct Staging {
   int E = 0;                   // elements per 128-byte-or-less smem row (ROW: points, COL: columns)
   int row_bytes = 0;
   int swz = 0;                 // XOR mask applied to bits 4.. from bits 7.. (0, 1, 3, 7)
+  // COL staging only: shared-memory row order of the points.  -1: natural;
+  // t >= 1: point bits [t, t + 3) form the lowest three row bits, then bits
+  // [0, t), then the rest (so that those bits select shared-memory banks).
+  int pmid = -1;
   uint32_t bytes() const { return (uint32_t)L * C * elem; }
   // Bytes one TMA box moves (less than bytes() when the column blocks of a
   // column staging are clamped to a pass with fewer columns than C).
@@ -53,7 +59,7 @@ struct Staging {
 };
 
 Staging make_staging(Kind kind, int L, int C, int elem, int64_t sp, int64_t sc, int64_t so,
-                     int64_t ncols, int64_t nouter);
+                     int64_t ncols, int64_t nouter, int pmid = -1);
 
 // A-operand byte offset of (row r, complex position n) in the SWIZZLE_64B
 // K-major layout (8-row atoms of 512 bytes).
@@ -77,6 +83,9 @@ struct PassLayout {
   // epilogue tables: per stage s, per row r: (dst_base >> 2) | (aux << 16)
   std::vector<uint32_t> epi_tab;    // [s][r]
   std::vector<uint32_t> kofs;       // [s][16] XOR offsets (bytes)
+  // Radix-R twiddle table layout in shared memory (tail_layout.h): -1
+  // natural (row items), t >= 0 folded with row order t (column items).
+  int tail_pm = -1;
   // bank-conflict figures (wavefronts actually used / ideal), for reports
   double prologue_excess = 0, epilogue_excess = 0;
   std::string describe() const;

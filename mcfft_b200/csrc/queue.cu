@@ -40,6 +40,7 @@ bool fill_qpass(const TilePass& tp, int dir, const void* in, void* out, QPass* q
   q->post_shift = a.post_shift;
   q->post_scale = a.post_scale;
   q->inverse = dir;
+  q->tail_pm = a.tail_pm;
   std::memcpy(q->in_cmul, a.in_cmul, sizeof(q->in_cmul));
   std::memcpy(q->in_omul, a.in_omul, sizeof(q->in_omul));
   std::memcpy(q->out_cmul, a.out_cmul, sizeof(q->out_cmul));

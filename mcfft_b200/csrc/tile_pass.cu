@@ -174,6 +174,7 @@ void fill_tile_args(TilePass* tp) {
     a.out_omul[d] = l.out.omul[d];
   }
   a.in_tile_bytes = l.in.box_bytes();
+  a.tail_pm = l.tail_pm;
   for (size_t i = 0; i < l.lofs.size() && i < 16; ++i) a.lofs[i] = l.lofs[i];
   for (size_t i = 0; i < l.sofs.size() && i < 32; ++i) a.sofs[i] = l.sofs[i];
   for (int s = 0; s < l.NST && s < kMaxStages; ++s)
