@@ -87,6 +87,11 @@ __device__ __forceinline__ void sts128(uint32_t addr, uint4 v) {
                "r"(v.w)
                : "memory");
 }
+__device__ __forceinline__ uint2 lds64(uint32_t addr) {
+  uint2 v;
+  asm volatile("ld.shared.v2.b32 {%0,%1}, [%2];" : "=r"(v.x), "=r"(v.y) : "r"(addr));
+  return v;
+}
 __device__ __forceinline__ void sts32(uint32_t addr, uint32_t v) {
   asm volatile("st.shared.b32 [%0], %1;" ::"r"(addr), "r"(v) : "memory");
 }
@@ -515,8 +520,11 @@ struct F16Tile {
         // column items (all four sub-vectors share the row)
         const uint32_t trow = ient[j].y & 0x7FFFFFFFu;
         const bool colitem = (ient[j].y >> 31) != 0;
-        // Sub-vector jj: radix-R butterflies, twiddles from row tw(jj), stores.
-        auto subvec = [&](int jj, auto tw_of) {
+        // Sub-vector jj: radix-R butterflies, twiddles W^(k v) / R (k = 0
+        // is exactly 1 / R, a power of two: output 0 is only scaled, and
+        // only entry 1 of the row's first chunk is read: tw1 = entry 1,
+        // tw_of(k2) = chunk k2), stores.
+        auto subvec = [&](int jj, uint2 tw1, auto tw_of) {
           __half2 hv[R];
 #pragma unroll
           for (int n = 0; n < R; ++n) {
@@ -524,30 +532,38 @@ struct F16Tile {
             hv[n] = *reinterpret_cast<const __half2*>(&w);
           }
           small_dft_h2<R>(hv, tsgn);
+          const __half2 y1 = h2cmul(hv[1], *reinterpret_cast<const __half2*>(&tw1.x),
+                                    *reinterpret_cast<const __half2*>(&tw1.y));
+          const __half2 y0 = __hmul2(hv[0], __float2half2_rn(1.f / R));
+          sts32w(xo(st, a.sofs[jj * R], x0), *reinterpret_cast<const uint32_t*>(&y0));
+          sts32w(xo(st, a.sofs[jj * R + 1], x0), *reinterpret_cast<const uint32_t*>(&y1));
 #pragma unroll
-          for (int k2 = 0; k2 < R / 2; ++k2) {
+          for (int k2 = 1; k2 < R / 2; ++k2) {
             const uint4 tw = tw_of(k2);
             const __half2 y0 = h2cmul(hv[2 * k2], *reinterpret_cast<const __half2*>(&tw.x),
                                       *reinterpret_cast<const __half2*>(&tw.y));
-            const __half2 y1 = h2cmul(hv[2 * k2 + 1], *reinterpret_cast<const __half2*>(&tw.z),
+            const __half2 y2 = h2cmul(hv[2 * k2 + 1], *reinterpret_cast<const __half2*>(&tw.z),
                                       *reinterpret_cast<const __half2*>(&tw.w));
             sts32w(xo(st, a.sofs[jj * R + 2 * k2], x0), *reinterpret_cast<const uint32_t*>(&y0));
-            sts32w(xo(st, a.sofs[jj * R + 2 * k2 + 1], x0), *reinterpret_cast<const uint32_t*>(&y1));
+            sts32w(xo(st, a.sofs[jj * R + 2 * k2 + 1], x0), *reinterpret_cast<const uint32_t*>(&y2));
           }
         };
         if (colitem) {
           // column items (folded table): the four sub-vectors share one
           // twiddle row
+          const uint2 tc1 = tile::lds64(x.sTail + tail_offset(trow, 1, R));
           uint4 twc[R / 2];
 #pragma unroll
-          for (int k2 = 0; k2 < R / 2; ++k2)
+          for (int k2 = 1; k2 < R / 2; ++k2)
             twc[k2] = tile::lds128(x.sTail + tail_offset(trow, 2 * k2, R));
 #pragma unroll
-          for (int jj = 0; jj < 4; ++jj) subvec(jj, [&](int k2) { return twc[k2]; });
+          for (int jj = 0; jj < 4; ++jj) subvec(jj, tc1, [&](int k2) { return twc[k2]; });
         } else {
 #pragma unroll
-          for (int jj = 0; jj < 4; ++jj)
-            subvec(jj, [&](int k2) { return tile::lds128(x.sTail + (trow + jj) * (R * 8) + 16 * k2); });
+          for (int jj = 0; jj < 4; ++jj) {
+            const uint32_t row = x.sTail + (trow + jj) * (R * 8);
+            subvec(jj, tile::lds64(row + 8), [&](int k2) { return tile::lds128(row + 16 * k2); });
+          }
         }
       }
     }

@@ -276,16 +276,21 @@ struct SplitTile {
           small_dft<R>(x, tsgn);
 #pragma unroll
           for (int k = 0; k < R; ++k) {
+            // entry 0 of the table is W^0 / R = 1 / R: output 0 only takes
+            // the (power-of-two) scale sc / R
             uint32_t hi, lo;
-            split2(cmulf(x[k], tw_of(k)), hi, lo);
+            split2(k == 0 ? make_float2(x[0].x * (sc * (1.f / R)), x[0].y * (sc * (1.f / R)))
+                          : cmulf(x[k], tw_of(k)),
+                   hi, lo);
             sts32_hl<T::HALF>(xo(st, a.sofs[sv * R + k], x0), hi, lo);
           }
         };
         if (colitem) {
           // column items: the sub-vectors share one twiddle row
           float2 wc[R];
+          wc[0] = make_float2(sc, 0.f);  // unused (entry 0 is 1 / R)
 #pragma unroll
-          for (int k = 0; k < R; ++k) {
+          for (int k = 1; k < R; ++k) {
             const float2 w = lds64f(x.t.sTail + tail_offset(trow, k, R));
             wc[k] = make_float2(w.x * sc, w.y * sc);
           }
