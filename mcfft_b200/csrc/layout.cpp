@@ -120,6 +120,27 @@ Staging make_staging(Kind kind, int L, int C, int elem, int64_t sp, int64_t sc, 
   s.C = C;
   s.elem = elem;
   const int per_row = 128 / elem;
+  if (kind == COL && pmid >= 1 && C > per_row) {
+    // Permuted point order with C / E > 1 column groups of E = 128 / elem
+    // (t = lg L - 3, so that the point bits above t + 3 are empty and the
+    // box fits five dims): column-low, point bits [t, t+3), [0, t),
+    // column-high, outer.
+    s.pmid = pmid;
+    s.E = per_row;
+    s.row_bytes = 128;
+    s.swz = swz_for(s.row_bytes);
+    const uint64_t nlo = uint64_t(1) << pmid;
+    s.ndims = 5;
+    s.gdim[0] = (uint64_t)s.E;             s.box[0] = (uint32_t)s.E;
+    s.gdim[1] = 8;                         s.box[1] = 8;              s.gstride_bytes[1] = nlo * sp * elem;
+    s.gdim[2] = nlo;                       s.box[2] = (uint32_t)nlo;  s.gstride_bytes[2] = (uint64_t)sp * elem;
+    s.gdim[3] = (uint64_t)(ncols / s.E);   s.box[3] = (uint32_t)(C / s.E); s.gstride_bytes[3] = (uint64_t)s.E * elem;
+    s.gdim[4] = (uint64_t)nouter;          s.box[4] = 1;              s.gstride_bytes[4] = (uint64_t)so * elem;
+    s.cmul[3] = C / s.E;
+    s.omul[4] = 1;
+    if (nouter <= 1) s.ndims = 4;
+    return s;
+  }
   if (kind == COL && pmid >= 1) {
     // Permuted point order (see Staging::pmid): all C columns in one
     // shared-memory row; dims columns, point bits [t, t+3), [0, t), the
@@ -486,7 +507,10 @@ bool build(PassLayout* pl, int L, int R, int C, Kind in_kind, Kind out_kind, int
   // Column input that can use a permuted staging (below) needs more
   // choices for the bits of A row 0..2: the prologue's stores decide among
   // the epilogue-optimal maps.
-  const bool permutable = in_kind == COL && C * in_elem <= 128 && ncols >= C;
+  // (all C columns in one 128-byte row, or, for R = 1, groups of them with
+  // t = lg L - 3)
+  const bool permutable =
+      in_kind == COL && ncols >= C && ilog2(L) >= 4 && (C * in_elem <= 128 || R == 1);
   const int xcap = permutable ? 64 : 12, ycap = permutable ? 8 : 24;
   for (int ix = 0; ix < (nst > 1 ? (int)xs.size() : 1) && xzero < xcap; ++ix) {
     std::vector<RowMap> maps;
@@ -575,7 +599,7 @@ bool build(PassLayout* pl, int L, int R, int C, Kind in_kind, Kind out_kind, int
   // banks -- then, unless that layout is conflict-free, the natural order,
   // which wins ties.
   std::vector<int> pmids = {-1};
-  const int tstar = ilog2(L / R) - 4;
+  const int tstar = C * in_elem <= 128 ? ilog2(L / R) - 4 : ilog2(L) - 3;
   if (permutable && tstar >= 1 && tstar <= ilog2(L) - 3) pmids.insert(pmids.begin(), tstar);
   double total_best = 1e30;
   std::vector<int> porder_best;
