@@ -1,0 +1,65 @@
+// Host-side check of the pass layout engine (mcfft_b200/csrc/layout.cpp),
+// compiled and run by tests/test_layout.py: for a pass shape given on the
+// command line it builds the layout and prints its bank-conflict figures,
+// the staging order and the twiddle-table mode, then verifies on the host
+// that the tables are consistent -- every A-operand slot of stage 0 is
+// written exactly once by the prologue, every staging slot is read once,
+// and the column items' twiddle rows land on the physical rows the folded
+// table stores them at.
+#include <cstdio>
+#include <cstdlib>
+#include <set>
+#include <string>
+#include <vector>
+
+#include "../mcfft_b200/csrc/layout.h"
+
+using namespace mcfft;
+using namespace mcfft::layout;
+
+int main(int argc, char** argv) {
+  if (argc != 6) {
+    std::fprintf(stderr, "usage: layout_check L R C in(row|col) out(row|col)\n");
+    return 2;
+  }
+  const int L = std::atoi(argv[1]), R = std::atoi(argv[2]), C = std::atoi(argv[3]);
+  const Kind ik = std::string(argv[4]) == "col" ? COL : ROW;
+  const Kind ok = std::string(argv[5]) == "col" ? COL : ROW;
+  const int64_t nc = 1024, nouter = 16;
+  // column layout: columns contiguous, points strided by nc; row layout: points contiguous
+  const int64_t isp = ik == COL ? nc : 1, isc = ik == COL ? 1 : L, iso = (int64_t)L * nc;
+  const int64_t osp = ok == COL ? nc : 1, osc = ok == COL ? 1 : L, oso = (int64_t)L * nc;
+  PassLayout pl;
+  std::string err;
+  if (!build(&pl, L, R, C, ik, ok, 4, 4, isp, isc, iso, osp, osc, oso, nc, nouter, &err)) {
+    std::printf("error %s\n", err.c_str());
+    return 1;
+  }
+  std::printf("prologue_excess %.3f\nepilogue_excess %.3f\npmid %d\ntail_pm %d\nin_ndims %d\n",
+              pl.prologue_excess, pl.epilogue_excess, pl.in.pmid, pl.tail_pm, pl.in.ndims);
+  // staging slots read by the prologue loads: each 16-byte slot once
+  std::set<uint32_t> loads, stores;
+  bool ok_tabs = true;
+  for (int it = 0; it < pl.items; ++it) {
+    const uint32_t lb = (pl.item_tab[2 * it] & 0xFFFFu) << 2, sb = (pl.item_tab[2 * it] >> 16) << 2;
+    for (uint32_t o : pl.lofs) ok_tabs &= loads.insert((lb ^ o) >> 4).second;
+    for (uint32_t o : pl.sofs) ok_tabs &= stores.insert((sb ^ o) >> (R == 1 ? 4 : 2)).second;
+  }
+  const size_t slots = (size_t)L * C * 4 / 16;
+  ok_tabs &= loads.size() == slots;
+  ok_tabs &= stores.size() == (R == 1 ? slots : slots * 4);
+  // column items: twiddle row = tail_row(v, tail_pm) of some v < L / R, all rows used
+  if (R > 1 && ik == COL) {
+    std::set<uint32_t> rows;
+    for (int it = 0; it < pl.items; ++it) {
+      const uint32_t w = pl.item_tab[2 * it + 1];
+      ok_tabs &= (w >> 31) != 0;
+      rows.insert(w & 0x7FFFFFFFu);
+    }
+    std::set<uint32_t> want;
+    for (uint32_t v = 0; v < (uint32_t)(L / R); ++v) want.insert(tail_row(v, pl.tail_pm));
+    ok_tabs &= rows == want;
+  }
+  std::printf("tables_consistent %d\n", ok_tabs ? 1 : 0);
+  return 0;
+}
