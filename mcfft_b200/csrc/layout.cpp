@@ -460,7 +460,7 @@ bool build(PassLayout* pl, int L, int R, int C, Kind in_kind, Kind out_kind, int
     // last-stage low bits: 5 bits from a small pool (c bits and low v bits)
     std::vector<int> pool;
     for (int j = 0; j < std::min(x.g, 7); ++j) pool.push_back(kC + j);
-    for (int j = 0; j < std::min(x.b, 4); ++j) pool.push_back(j);
+    for (int j = 0; j < std::min(x.b, 5); ++j) pool.push_back(j);
     std::vector<std::vector<int>> cands;
     const int n = (int)pool.size();
     for (int m = 0; m < (1 << n); ++m) {
