@@ -18,10 +18,11 @@ using namespace mcfft;
 using namespace mcfft::layout;
 
 int main(int argc, char** argv) {
-  if (argc != 6) {
-    std::fprintf(stderr, "usage: layout_check L R C in(row|col) out(row|col)\n");
+  if (argc != 6 && argc != 8) {
+    std::fprintf(stderr, "usage: layout_check L R C in(row|col) out(row|col) [in_elem out_elem]\n");
     return 2;
   }
+  const int ie = argc == 8 ? std::atoi(argv[6]) : 4, oe = argc == 8 ? std::atoi(argv[7]) : 4;
   const int L = std::atoi(argv[1]), R = std::atoi(argv[2]), C = std::atoi(argv[3]);
   const Kind ik = std::string(argv[4]) == "col" ? COL : ROW;
   const Kind ok = std::string(argv[5]) == "col" ? COL : ROW;
@@ -31,7 +32,7 @@ int main(int argc, char** argv) {
   const int64_t osp = ok == COL ? nc : 1, osc = ok == COL ? 1 : L, oso = (int64_t)L * nc;
   PassLayout pl;
   std::string err;
-  if (!build(&pl, L, R, C, ik, ok, 4, 4, isp, isc, iso, osp, osc, oso, nc, nouter, &err)) {
+  if (!build(&pl, L, R, C, ik, ok, ie, oe, isp, isc, iso, osp, osc, oso, nc, nouter, &err)) {
     std::printf("error %s\n", err.c_str());
     return 1;
   }
@@ -45,9 +46,10 @@ int main(int argc, char** argv) {
     for (uint32_t o : pl.lofs) ok_tabs &= loads.insert((lb ^ o) >> 4).second;
     for (uint32_t o : pl.sofs) ok_tabs &= stores.insert((sb ^ o) >> (R == 1 ? 4 : 2)).second;
   }
-  const size_t slots = (size_t)L * C * 4 / 16;
-  ok_tabs &= loads.size() == slots;
-  ok_tabs &= stores.size() == (R == 1 ? slots : slots * 4);
+  // staging: L C elements of ie bytes; A operand (hi): L C FP16 complex
+  const size_t in_slots = (size_t)L * C * ie / 16, a_slots = (size_t)L * C * 4 / 16;
+  ok_tabs &= loads.size() == in_slots;
+  ok_tabs &= stores.size() == (R == 1 ? a_slots : a_slots * 4);
   // column items: twiddle row = tail_row(v, tail_pm) of some v < L / R, all rows used
   if (R > 1 && ik == COL) {
     std::set<uint32_t> rows;
