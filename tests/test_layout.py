@@ -61,3 +61,27 @@ def test_layout_conflicts_and_tables(checker, L, R, C, ik, ok):
         assert int(out["tail_pm"]) == (int(out["pmid"]) if R > 1 else -1)
     if ik == "row":
         assert int(out["pmid"]) == -1 and int(out["tail_pm"]) == -1
+
+
+SPLIT_SHAPES = [  # L, R, C (8K-point tiles of the split form)
+    (64, 4, 128), (128, 8, 64), (256, 1, 32), (512, 2, 16), (1024, 4, 8), (2048, 8, 4),
+]
+
+
+@pytest.mark.parametrize("L,R,C", SPLIT_SHAPES)
+@pytest.mark.parametrize("ik,ok,ie", [("col", "col", 8), ("row", "col", 8), ("row", "row", 8),
+                                      ("col", "col", 4), ("row", "row", 4)])
+def test_split_layouts(checker, L, R, C, ik, ok, ie):
+    """Split form: FP32 (or FP16) staging in, FP32 out.  Tables consistent,
+    epilogue conflict-free; the passes of the 1D 2^20 workload (FP16 column
+    input, FP32 row input) also have a conflict-free prologue."""
+    r = subprocess.run([checker, str(L), str(R), str(C), ik, ok, str(ie), "8"],
+                       capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stdout + r.stderr
+    out = dict(line.split(None, 1) for line in r.stdout.splitlines())
+    assert out["tables_consistent"] == "1"
+    assert float(out["epilogue_excess"]) == pytest.approx(0.0, abs=1e-9)
+    pro = float(out["prologue_excess"])
+    assert pro <= 1.5 + 1e-9
+    if L == 1024 or L == 512:
+        assert pro == pytest.approx(0.0, abs=1e-9)
