@@ -512,57 +512,77 @@ struct F16Tile {
         for (int n = 0; n < R; ++n) q[j][n] = lds128w(xo(lb, a.lofs[n], bb));
       }
       if (INPLACE_PROLOGUE) tile::named_bar(1, NCT);
-#pragma unroll
-      for (int j = 0; j < NIT_P; ++j) {
-        if (S::ITEMS % NCT != 0 && ctid + j * NCT >= S::ITEMS) break;
+      // Sub-vector jj of item j: radix-R butterflies, twiddles W^(k v) / R
+      // (k = 0 is exactly 1 / R, a power of two: output 0 is only scaled,
+      // and only entry 1 of the row's first chunk is read: tw1 = entry 1,
+      // tw_of(k2) = chunk k2), stores.
+      auto subvec = [&](int j, int jj, uint2 tw1, auto tw_of) {
         const uint32_t st = (ient[j].x >> 16) << 2;
-        // item word 1: tail twiddle row of sub-vector 0; bit 31 set for
-        // column items (all four sub-vectors share the row)
-        const uint32_t trow = ient[j].y & 0x7FFFFFFFu;
-        const bool colitem = (ient[j].y >> 31) != 0;
-        // Sub-vector jj: radix-R butterflies, twiddles W^(k v) / R (k = 0
-        // is exactly 1 / R, a power of two: output 0 is only scaled, and
-        // only entry 1 of the row's first chunk is read: tw1 = entry 1,
-        // tw_of(k2) = chunk k2), stores.
-        auto subvec = [&](int jj, uint2 tw1, auto tw_of) {
-          __half2 hv[R];
+        __half2 hv[R];
 #pragma unroll
-          for (int n = 0; n < R; ++n) {
-            const uint32_t w = jj == 0 ? q[j][n].x : jj == 1 ? q[j][n].y : jj == 2 ? q[j][n].z : q[j][n].w;
-            hv[n] = *reinterpret_cast<const __half2*>(&w);
-          }
-          small_dft_h2<R>(hv, tsgn);
-          const __half2 y1 = h2cmul(hv[1], *reinterpret_cast<const __half2*>(&tw1.x),
-                                    *reinterpret_cast<const __half2*>(&tw1.y));
-          const __half2 y0 = __hmul2(hv[0], __float2half2_rn(1.f / R));
-          sts32w(xo(st, a.sofs[jj * R], x0), *reinterpret_cast<const uint32_t*>(&y0));
-          sts32w(xo(st, a.sofs[jj * R + 1], x0), *reinterpret_cast<const uint32_t*>(&y1));
+        for (int n = 0; n < R; ++n) {
+          const uint32_t w = jj == 0 ? q[j][n].x : jj == 1 ? q[j][n].y : jj == 2 ? q[j][n].z : q[j][n].w;
+          hv[n] = *reinterpret_cast<const __half2*>(&w);
+        }
+        small_dft_h2<R>(hv, tsgn);
+        const __half2 y1 = h2cmul(hv[1], *reinterpret_cast<const __half2*>(&tw1.x),
+                                  *reinterpret_cast<const __half2*>(&tw1.y));
+        const __half2 y0 = __hmul2(hv[0], __float2half2_rn(1.f / R));
+        sts32w(xo(st, a.sofs[jj * R], x0), *reinterpret_cast<const uint32_t*>(&y0));
+        sts32w(xo(st, a.sofs[jj * R + 1], x0), *reinterpret_cast<const uint32_t*>(&y1));
 #pragma unroll
-          for (int k2 = 1; k2 < R / 2; ++k2) {
-            const uint4 tw = tw_of(k2);
-            const __half2 y0 = h2cmul(hv[2 * k2], *reinterpret_cast<const __half2*>(&tw.x),
-                                      *reinterpret_cast<const __half2*>(&tw.y));
-            const __half2 y2 = h2cmul(hv[2 * k2 + 1], *reinterpret_cast<const __half2*>(&tw.z),
-                                      *reinterpret_cast<const __half2*>(&tw.w));
-            sts32w(xo(st, a.sofs[jj * R + 2 * k2], x0), *reinterpret_cast<const uint32_t*>(&y0));
-            sts32w(xo(st, a.sofs[jj * R + 2 * k2 + 1], x0), *reinterpret_cast<const uint32_t*>(&y2));
-          }
-        };
-        if (colitem) {
-          // column items (folded table): the four sub-vectors share one
-          // twiddle row
-          const uint2 tc1 = tile::lds64(x.sTail + tail_offset(trow, 1, R));
-          uint4 twc[R / 2];
+        for (int k2 = 1; k2 < R / 2; ++k2) {
+          const uint4 tw = tw_of(k2);
+          const __half2 z0 = h2cmul(hv[2 * k2], *reinterpret_cast<const __half2*>(&tw.x),
+                                    *reinterpret_cast<const __half2*>(&tw.y));
+          const __half2 z1 = h2cmul(hv[2 * k2 + 1], *reinterpret_cast<const __half2*>(&tw.z),
+                                    *reinterpret_cast<const __half2*>(&tw.w));
+          sts32w(xo(st, a.sofs[jj * R + 2 * k2], x0), *reinterpret_cast<const uint32_t*>(&z0));
+          sts32w(xo(st, a.sofs[jj * R + 2 * k2 + 1], x0), *reinterpret_cast<const uint32_t*>(&z1));
+        }
+      };
+      constexpr int HP = NIT_P / 2;
+      if (NIT_P % 2 == 0 && S::ITEMS % NCT == 0 && a.tail_pm == kTailNaturalPaired) {
+        // Row items whose pairs (j, j + NIT_P / 2) read the same twiddle
+        // rows (the layout guarantees it): each row is loaded once.
 #pragma unroll
-          for (int k2 = 1; k2 < R / 2; ++k2)
-            twc[k2] = tile::lds128(x.sTail + tail_offset(trow, 2 * k2, R));
-#pragma unroll
-          for (int jj = 0; jj < 4; ++jj) subvec(jj, tc1, [&](int k2) { return twc[k2]; });
-        } else {
+        for (int j = 0; j < HP; ++j) {
+          const uint32_t trow = ient[j].y & 0x7FFFFFFFu;
 #pragma unroll
           for (int jj = 0; jj < 4; ++jj) {
             const uint32_t row = x.sTail + (trow + jj) * (R * 8);
-            subvec(jj, tile::lds64(row + 8), [&](int k2) { return tile::lds128(row + 16 * k2); });
+            const uint2 tw1 = tile::lds64(row + 8);
+            uint4 twr[R / 2];
+#pragma unroll
+            for (int k2 = 1; k2 < R / 2; ++k2) twr[k2] = tile::lds128(row + 16 * k2);
+            subvec(j, jj, tw1, [&](int k2) { return twr[k2]; });
+            subvec(j + HP, jj, tw1, [&](int k2) { return twr[k2]; });
+          }
+        }
+      } else {
+#pragma unroll
+        for (int j = 0; j < NIT_P; ++j) {
+          if (S::ITEMS % NCT != 0 && ctid + j * NCT >= S::ITEMS) break;
+          // item word 1: tail twiddle row of sub-vector 0; bit 31 set for
+          // column items (all four sub-vectors share the row)
+          const uint32_t trow = ient[j].y & 0x7FFFFFFFu;
+          const bool colitem = (ient[j].y >> 31) != 0;
+          if (colitem) {
+            // column items (folded table): the four sub-vectors share one
+            // twiddle row
+            const uint2 tc1 = tile::lds64(x.sTail + tail_offset(trow, 1, R));
+            uint4 twc[R / 2];
+#pragma unroll
+            for (int k2 = 1; k2 < R / 2; ++k2)
+              twc[k2] = tile::lds128(x.sTail + tail_offset(trow, 2 * k2, R));
+#pragma unroll
+            for (int jj = 0; jj < 4; ++jj) subvec(j, jj, tc1, [&](int k2) { return twc[k2]; });
+          } else {
+#pragma unroll
+            for (int jj = 0; jj < 4; ++jj) {
+              const uint32_t row = x.sTail + (trow + jj) * (R * 8);
+              subvec(j, jj, tile::lds64(row + 8), [&](int k2) { return tile::lds128(row + 16 * k2); });
+            }
           }
         }
       }

@@ -655,12 +655,31 @@ bool build(PassLayout* pl, int L, int R, int C, Kind in_kind, Kind out_kind, int
   p.in = in_best;
   p.tail_pm = (in_kind == COL && R > 1) ? std::max(p.in.pmid, 0) : -1;
   if (porder_best.empty()) { *err = "no linear prologue"; return false; }
+  // Row items of R > 1: the bits above the lane bits only decide which warp
+  // and which of its two items a thread gets (conflicts depend on the lane
+  // bits alone).  Put a column bit on top, so that a thread's two items
+  // (item indices i and i + half the items) differ only in their column and
+  // read the same radix-R twiddle rows, which the kernel then loads once.
+  bool paired = false;
+  if (R > 1 && in_kind == ROW && nb > nl) {
+    std::vector<int> high(porder_best.begin() + nl, porder_best.end());
+    int pick = -1;
+    for (int b : high)
+      if (b < x.g) pick = b;  // field 0 = column bits
+    if (pick >= 0) {
+      high.erase(std::find(high.begin(), high.end(), pick));
+      high.push_back(pick);
+      std::copy(high.begin(), high.end(), porder_best.begin() + nl);
+      paired = true;
+    }
+  }
   std::vector<RowMap> best_maps = maps_best;
   {
     bool lin = true;
     p.prologue_excess = eval_prologue(x, best_maps[0], porder_best, true, &lin);
     if (!lin) { *err = "prologue offsets are not XOR-linear"; return false; }
   }
+  if (paired) p.tail_pm = kTailNaturalPaired;
   p.epi_tab.assign((size_t)nst * p.NROWS, 0);
   p.kofs.assign((size_t)nst * 16, 0);
   double e = 0;

@@ -2,8 +2,10 @@
 // tile pass, shared by the host layout engine (which writes the row of each
 // column item into its table) and the kernels (which fill and read it).
 //
-// Natural layout (row-item passes): entry (v, k), k < R, of 8 bytes at
-// 8 (R v + k).  Folded layout (column-item passes, tail_pm = t >= 0): row v
+// Natural layout (row-item passes, tail_pm < 0): entry (v, k), k < R, of 8
+// bytes at 8 (R v + k); tail_pm = kTailNaturalPaired (-2) also says that the
+// two prologue items of a thread (item indices i and i + items / 2) read the
+// same rows.  Folded layout (column-item passes, tail_pm = t >= 0): row v
 // at tail_row(v, t), which puts bits [t, t + 3) of v lowest (t = 0 keeps v),
 // and within a row of R / 2 chunks of 16 bytes chunk k / 2 at
 // (k / 2) ^ (row >> (3 - log2(R / 2)) & (R / 2 - 1)): the rows the eight
@@ -19,6 +21,9 @@
 #endif
 
 namespace mcfft {
+
+constexpr int kTailNatural = -1;
+constexpr int kTailNaturalPaired = -2;
 
 MCFFT_HD uint32_t tail_row(uint32_t v, int t) {
   if (t <= 0) return v;

@@ -5,7 +5,7 @@
 // that the tables are consistent -- every A-operand slot of stage 0 is
 // written exactly once by the prologue, every staging slot is read once,
 // and the column items' twiddle rows land on the physical rows the folded
-// table stores them at.
+// table stores them at, and that paired row items share their rows.
 #include <cstdio>
 #include <cstdlib>
 #include <set>
@@ -62,6 +62,10 @@ int main(int argc, char** argv) {
     for (uint32_t v = 0; v < (uint32_t)(L / R); ++v) want.insert(tail_row(v, pl.tail_pm));
     ok_tabs &= rows == want;
   }
+  // paired row items: items i and i + items / 2 read the same twiddle rows
+  if (pl.tail_pm == kTailNaturalPaired)
+    for (int it = 0; it < pl.items / 2; ++it)
+      ok_tabs &= pl.item_tab[2 * it + 1] == pl.item_tab[2 * (it + pl.items / 2) + 1];
   std::printf("tables_consistent %d\n", ok_tabs ? 1 : 0);
   return 0;
 }
