@@ -602,11 +602,13 @@ struct F16Tile {
     constexpr uint32_t IDESC = sm100::idesc_f16_f32(128, 32);
     const uint32_t sb = b ? x.sS1 : x.sS0;
     const uint32_t xs = ((S::NST - s) & 1) ? x.sA : sb;  // this stage's operand
-    // Each M-tile's two MMAs and its commit are issued by lane 0 of the
-    // sub-partition-0 warp that drains that M-tile, so four warps issue
-    // in parallel (a single issuing thread serialises ~100 cycles per
-    // tcgen05.mma).  tcgen05.commit tracks the issuing thread's MMAs.
-    if (sp == 0 && lane == 0) {
+    // Each M-tile's two MMAs and its commit are issued by lane 0 of one of
+    // the four warps that drain that M-tile -- the one on sub-partition
+    // (warp / 4) % 4, so that the issuing warps sit on all four SM
+    // sub-partitions and issue in parallel (one thread serialises its
+    // tcgen05.mma instructions).  tcgen05.commit tracks the issuing thread's
+    // MMAs.
+    if (sp == ((warp >> 2) & 3) && lane == 0) {
 #pragma unroll
       for (int j = 0; j < NIT_E; ++j) {
         const uint32_t m = (warp >> 2) + j * (NCW / 4);

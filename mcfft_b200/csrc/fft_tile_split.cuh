@@ -316,7 +316,7 @@ struct SplitTile {
     for (int s = 0; s < S::NST; ++s) {
       const uint32_t xs = ((S::NST - s) & 1) ? x.t.sA : sb;   // this stage's operand (hi)
       const uint32_t xn = ((S::NST - s) & 1) ? bb : x.t.bA;   // next stage's operand (window-relative)
-      if (sp == 0 && lane == 0) {
+      if (sp == ((warp >> 2) & 3) && lane == 0) {  // issuers on all four sub-partitions
 #pragma unroll
         for (int j = 0; j < NIT_E; ++j) {
           const uint32_t m = (warp >> 2) + j * (NCW / 4);
