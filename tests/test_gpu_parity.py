@@ -25,7 +25,7 @@ SPLIT_TOL = 2e-6
 
 SIZES_1D = [(16, 256), (32, 128), (64, 256), (128, 128), (256, 64), (512, 32), (1024, 16),
             (2048, 8), (4096, 256), (8192, 4), (16384, 2), (32768, 2), (65536, 1),
-            (1 << 20, 2)]
+            (1 << 20, 2), (1 << 22, 1)]
 
 
 @pytest.mark.parametrize("n,batch", SIZES_1D)
@@ -61,7 +61,7 @@ def test_split_1d_f16_input(n, batch):
 
 @pytest.mark.parametrize("prec", [mc.PREC_FP16, mc.PREC_SPLIT])
 @pytest.mark.parametrize("nx,ny,batch", [(16, 16, 4), (128, 256, 2), (256, 128, 2), (512, 512, 1),
-                                         (1024, 1024, 1), (64, 2048, 1)])
+                                         (1024, 1024, 1), (64, 2048, 1), (2048, 256, 1)])
 def test_2d(prec, nx, ny, batch):
     f16 = prec == mc.PREC_FP16
     x = rand_complex((batch, nx, ny), seed=nx + ny)
@@ -82,7 +82,7 @@ def test_2d_wide_range_split():
 
 
 @pytest.mark.parametrize("prec", [mc.PREC_FP16, mc.PREC_SPLIT])
-@pytest.mark.parametrize("dims", [(16, 16, 16), (32, 64, 128), (64, 64, 64)])
+@pytest.mark.parametrize("dims", [(16, 16, 16), (32, 64, 128), (64, 64, 64), (256, 256, 32)])
 def test_3d(prec, dims):
     f16 = prec == mc.PREC_FP16
     x = rand_complex((1,) + dims, seed=3)
