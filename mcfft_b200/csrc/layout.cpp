@@ -8,6 +8,7 @@
 #include <map>
 #include <set>
 #include <sstream>
+#include <thread>
 
 namespace mcfft {
 namespace layout {
@@ -198,6 +199,34 @@ Staging make_staging(Kind kind, int L, int C, int elem, int64_t sp, int64_t sc, 
 }
 
 namespace {
+
+// Host threads for the layout search (MCFFT_LAYOUT_THREADS overrides; 1
+// searches on the calling thread only).
+size_t search_threads() {
+  static const size_t n = [] {
+    if (const char* e = std::getenv("MCFFT_LAYOUT_THREADS")) return (size_t)std::max(1, std::atoi(e));
+    const unsigned h = std::thread::hardware_concurrency();
+    return (size_t)std::min(16u, std::max(1u, h));
+  }();
+  return n;
+}
+
+// Runs fn(i) for i in [0, n) on the search threads.
+template <class F>
+void parallel_for(size_t n, F fn) {
+  const size_t nthr = std::min(search_threads(), n);
+  if (nthr <= 1) {
+    for (size_t i = 0; i < n; ++i) fn(i);
+    return;
+  }
+  auto work = [&](size_t t) {
+    for (size_t i = t; i < n; i += nthr) fn(i);
+  };
+  std::vector<std::thread> pool;
+  for (size_t t = 1; t < nthr; ++t) pool.emplace_back(work, t);
+  work(0);
+  for (auto& th : pool) th.join();
+}
 
 struct Ctx {
   PassLayout* pl;
@@ -524,29 +553,46 @@ bool build(PassLayout* pl, int L, int R, int C, Kind in_kind, Kind out_kind, int
     xr.push_back({c, ix});
     if (c < 1e-9) ++xzero;
   }
-  for (int iy = 0; iy < (int)ys.size() && yzero < 24; ++iy) {
-    std::vector<RowMap> maps;
-    if (!maps_for(xs.empty() ? std::vector<int>{} : xs[0], ys[iy], &maps)) continue;
-    bool lin = true;
-    double c = eval_epilogue(x, maps, nst - 1, false, nullptr, nullptr, &lin);
-    if (!lin) continue;
-    yr.push_back({c, iy});
-    if (c < 1e-9) ++yzero;
+  // last-stage candidates, evaluated in chunks in parallel and taken in
+  // order until 24 conflict-free ones are found (as a sequential scan would)
+  for (size_t c0 = 0; c0 < ys.size() && yzero < 24; c0 += 64) {
+    const size_t cn = std::min<size_t>(64, ys.size() - c0);
+    std::vector<double> cost(cn, 0.0);
+    std::vector<char> ok(cn, 0);
+    parallel_for(cn, [&](size_t k) {
+      std::vector<RowMap> maps;
+      if (!maps_for(xs.empty() ? std::vector<int>{} : xs[0], ys[c0 + k], &maps)) return;
+      bool lin = true;
+      cost[k] = eval_epilogue(x, maps, nst - 1, false, nullptr, nullptr, &lin);
+      ok[k] = lin;
+    });
+    for (size_t k = 0; k < cn && yzero < 24; ++k) {
+      if (!ok[k]) continue;
+      yr.push_back({cost[k], (int)(c0 + k)});
+      if (cost[k] < 1e-9) ++yzero;
+    }
   }
   std::sort(xr.begin(), xr.end());
   std::sort(yr.begin(), yr.end());
   struct Cand { double cost; std::vector<RowMap> maps; };
   std::vector<Cand> cands;
-  for (size_t i = 0; i < std::min<size_t>(xr.size(), xcap); ++i) {
-    for (size_t j = 0; j < std::min<size_t>(yr.size(), ycap); ++j) {
+  {
+    const size_t ni = std::min<size_t>(xr.size(), xcap), nj = std::min<size_t>(yr.size(), ycap);
+    std::vector<Cand> all(ni * nj);
+    std::vector<char> ok(ni * nj, 0);
+    parallel_for(ni * nj, [&](size_t k) {
+      const size_t i = k / nj, j = k % nj;
       std::vector<RowMap> maps;
-      if (!maps_for(xs[xr[i].second], ys[yr[j].second], &maps)) continue;
+      if (!maps_for(xs[xr[i].second], ys[yr[j].second], &maps)) return;
       double c = xr[i].first + yr[j].first;
       bool lin = true;
       if (nst > 1) c += eval_epilogue(x, maps, nst - 2, false, nullptr, nullptr, &lin);
-      if (!lin) continue;
-      cands.push_back({c, maps});
-    }
+      if (!lin) return;
+      all[k] = {c, maps};
+      ok[k] = 1;
+    });
+    for (size_t k = 0; k < ni * nj; ++k)
+      if (ok[k]) cands.push_back(std::move(all[k]));
   }
   if (cands.empty()) { *err = "no linear row map"; return false; }
   std::stable_sort(cands.begin(), cands.end(),
@@ -612,36 +658,60 @@ bool build(PassLayout* pl, int L, int R, int C, Kind in_kind, Kind out_kind, int
     for (size_t ci = 0; ci < std::min<size_t>(cands.size(), permutable ? 32 : 4); ++ci) {
       if (ci > 0 && cands[ci].cost > cands[0].cost + 1e-9) break;
       if (total_best <= cands[0].cost * epi_weight / 16.0 + 1e-9) break;  // found the optimum
+      // Candidate item orders: 5 lane bits from the pool (which 3 of them
+      // form the 8-lane phase), the other bits after them; evaluated in
+      // chunks on the host's threads and taken in enumeration order (the
+      // first of the cheapest wins; a conflict-free order ends the search),
+      // so the result does not depend on the thread count.
+      std::vector<std::vector<int>> orders;
+      {
+        std::vector<int> comb(nl);
+        std::function<void(int, int)> gen = [&](int start, int depth) {
+          if (depth == nl) {
+            for (int m = 0; m < (1 << nl); ++m) {
+              if (__builtin_popcount(m) != std::min(3, nl)) continue;
+              std::vector<int> order;
+              for (int i = 0; i < nl; ++i) if (m >> i & 1) order.push_back(comb[i]);
+              for (int i = 0; i < nl; ++i) if (!(m >> i & 1)) order.push_back(comb[i]);
+              std::set<int> u(order.begin(), order.end());
+              for (int i = 0; i < nb; ++i)
+                if (!u.count(i)) order.push_back(i);
+              orders.push_back(order);
+            }
+            return;
+          }
+          for (size_t i = start; i < lane_pool.size(); ++i) {
+            comb[depth] = lane_pool[i];
+            gen((int)i + 1, depth + 1);
+          }
+        };
+        gen(0, 0);
+      }
       double pbest = 1e30;
       std::vector<int> porder;
-      std::vector<int> comb(nl);
-      std::function<void(int, int)> rec = [&](int start, int depth) {
-        if (pbest < 1e-9) return;
-        if (depth == nl) {
-          // which 3 of the 5 lane bits form the 8-lane phase
-          for (int m = 0; m < (1 << nl) && pbest > 1e-9; ++m) {
-            if (__builtin_popcount(m) != std::min(3, nl)) continue;
-            std::vector<int> order;
-            for (int i = 0; i < nl; ++i) if (m >> i & 1) order.push_back(comb[i]);
-            for (int i = 0; i < nl; ++i) if (!(m >> i & 1)) order.push_back(comb[i]);
-            std::set<int> u(order.begin(), order.end());
-            for (int i = 0; i < nb; ++i)
-              if (!u.count(i)) order.push_back(i);
-            bool lin = true;
-            double c = eval_prologue(x, cands[ci].maps[0], order, false, &lin);
-            if (lin && c < pbest - 1e-9) {
-              pbest = c;
-              porder = order;
-            }
+      const size_t nthr = search_threads();
+      const size_t chunk = 32 * nthr;
+      std::vector<double> cost(chunk);
+      std::vector<char> lin(chunk);
+      for (size_t c0 = 0; c0 < orders.size() && pbest > 1e-9; c0 += chunk) {
+        const size_t cn = std::min(chunk, orders.size() - c0);
+        auto work = [&](size_t t) {
+          for (size_t i = t; i < cn; i += nthr) {
+            bool l = true;
+            cost[i] = eval_prologue(x, cands[ci].maps[0], orders[c0 + i], false, &l);
+            lin[i] = l;
           }
-          return;
-        }
-        for (size_t i = start; i < lane_pool.size(); ++i) {
-          comb[depth] = lane_pool[i];
-          rec((int)i + 1, depth + 1);
-        }
-      };
-      rec(0, 0);
+        };
+        std::vector<std::thread> pool;
+        for (size_t t = 1; t < nthr; ++t) pool.emplace_back(work, t);
+        work(0);
+        for (auto& th : pool) th.join();
+        for (size_t i = 0; i < cn && pbest > 1e-9; ++i)
+          if (lin[i] && cost[i] < pbest - 1e-9) {
+            pbest = cost[i];
+            porder = orders[c0 + i];
+          }
+      }
       if (porder.empty()) continue;
       const double total = pbest + cands[ci].cost * epi_weight / 16.0;
       if (total < total_best - 1e-9 || (pm < 0 && total <= total_best + 1e-9)) {

@@ -28,7 +28,7 @@ def checker(tmp_path_factory):
     if not cxx:
         pytest.skip("no host C++ compiler")
     exe = str(tmp_path_factory.mktemp("layout") / "layout_check")
-    subprocess.run([cxx, "-O2", "-std=c++17", "-o", exe, os.path.join(HERE, "layout_check.cpp"),
+    subprocess.run([cxx, "-O2", "-std=c++17", "-pthread", "-o", exe, os.path.join(HERE, "layout_check.cpp"),
                     os.path.join(SRC, "layout.cpp")], check=True)
     return exe
 
