@@ -811,6 +811,10 @@ mcfftResult build_queue(mcfftPlan p) {
     }
   std::vector<QItem> items;
   const int64_t G = maxg;
+  // first-pass tiles per CTA queued at a time (a CTA reloads a pass's tables when its
+  // consecutive items switch pass)
+  int64_t QC = 16;
+  if (const char* e = std::getenv("MCFFT_QUEUE_CHUNK")) QC = std::max<int64_t>(1, std::atoll(e));
   for (size_t i = 0; i < np;) {
     size_t j = i;
     while (j < np && p->passes[j].grp == p->passes[i].grp) ++j;
@@ -819,10 +823,10 @@ mcfftResult build_queue(mcfftPlan p) {
     for (int l = 0; l < nl; ++l) tot[l] = p->passes[i + l].tp.args.ntiles;
     for (int l = 1; l < nl; ++l) {
       const Pass& P = p->passes[i + l - 1];
-      W[l] = std::max<int64_t>(1, (4 * G * P.sig_mul + P.sig_div - 1) / P.sig_div);
+      W[l] = std::max<int64_t>(1, (QC * G * P.sig_mul + P.sig_div - 1) / P.sig_div);
     }
     for (bool left = true; left;) {
-      for (int64_t c = 0; c < 4 * G && em[0] < tot[0]; ++c)
+      for (int64_t c = 0; c < QC * G && em[0] < tot[0]; ++c)
         items.push_back({(uint32_t)i, (uint32_t)em[0]++});
       for (int l = 1; l < nl; ++l) {
         const Pass& P = p->passes[i + l - 1];
