@@ -39,10 +39,13 @@ namespace mcfft {
 
 constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
-// Poll limit for mbarrier waits: far above any legitimate MMA latency
-// (microseconds), small enough that a lost arrival ends the kernel with an
-// error status within about a second instead of hanging the GPU.
-constexpr uint32_t kWaitLimit = 1u << 24;
+// Time limit, in nanoseconds of the global timer, for every wait in the
+// kernels (mbarrier phases, dependency counters): far above any legitimate
+// wait (microseconds for a load or an MMA, milliseconds for the largest
+// producing pass of a queued transform), short enough that a lost arrival
+// or an unmet dependency ends the kernel with an error status after about
+// one second instead of hanging the GPU.
+constexpr uint32_t kWaitLimit = 1000000000u;
 
 __host__ __device__ constexpr int ilog2c(int x) { return x <= 1 ? 0 : 1 + ilog2c(x >> 1); }
 __host__ __device__ constexpr int pow2ceil(int x) { return x <= 1 ? 1 : 2 * pow2ceil((x + 1) >> 1); }

@@ -19,7 +19,9 @@
 // queue so that every dependency points to an earlier item, the kernel is
 // launched cooperatively (all CTAs resident), and the producer never blocks
 // its own stores while it waits for a dependency, so every wait ends.  All
-// waits are bounded; on timeout the kernel records kStatusTimeout.
+// waits are bounded by kWaitLimit nanoseconds of global time; on timeout
+// the kernel records kStatusTimeout, drains its own copies in flight,
+// frees its tensor memory and returns.
 //
 // Memory ordering of a dependency: writer = bulk store, wait for its
 // completion (cp.async.bulk.wait_group 0), proxy fence, release add;
@@ -279,7 +281,8 @@ __global__ void __maxnreg__(96) fft_queue(const __grid_constant__ QArgs a) {
     if (lane == 0) {
       int64_t il = 0, is = 0;  // next local item to load / to store
       int64_t sig = -1;        // stored item whose completion is still to be signalled
-      uint32_t idle = 0;
+      bool idle = false;       // no progress since idle_since (global timer, ns)
+      uint32_t idle_since = 0;
       // Completion of a producing tile: its bulk store has finished writing,
       // then a release add on every key it covers.
       auto signal = [&](int64_t k) {
@@ -333,9 +336,14 @@ __global__ void __maxnreg__(96) fft_queue(const __grid_constant__ QArgs a) {
           sig = -1;
         }
         if (moved) {
-          idle = 0;
+          idle = false;
         } else {
-          if (*abort_flag || ++idle > kWaitLimit) {
+          const uint32_t now = sm100::globaltimer_ns();
+          if (!idle) {
+            idle = true;
+            idle_since = now;
+          }
+          if (*abort_flag || now - idle_since > kWaitLimit) {
             *abort_flag = 1;
             break;
           }

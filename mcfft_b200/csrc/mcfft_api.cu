@@ -25,6 +25,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdint>
 #include <cstdlib>
 #include <cstring>
 #include <mutex>
@@ -90,6 +91,11 @@ struct Queue {
   std::vector<int> wait_base, sig_base;  // per pass
   int grid = 0;
   QArgs* args = nullptr;  // host staging of the parameter block
+  // Fault injection for the failure-detection tests (MCFFT_INJECT_STALL at
+  // plan time): every dependent pass waits for a producer count that can
+  // never be reached, so its tiles time out on the device and the exec
+  // reports MCFFT_DEVICE_TIMEOUT.  Host-side only; nothing faults.
+  bool stall = false;
 };
 
 }  // namespace
@@ -779,8 +785,8 @@ mcfftResult build_group(mcfftPlan p, int ndim, const int64_t* dims, int64_t batc
 // shape is faster that way: each pass kernel keeps its tables in its
 // parameter block).
 // Queue order: per transform group, the first pass's tiles in chunks of
-// four per CTA, each later pass's tile for key k once the previous pass's
-// tiles for keys up to k + W are queued (W ~ four tiles per CTA of lag), so
+// QC (sixteen) per CTA, each later pass's tile for key k once the previous
+// pass's tiles for keys up to k + W are queued (W ~ QC tiles per CTA of lag), so
 // every dependency points backwards, a CTA runs several tiles of one pass
 // in a row (its tables stay in shared memory), and the intermediate is read
 // back while it is in L2.
@@ -855,6 +861,7 @@ mcfftResult build_queue(mcfftPlan p) {
   q.grid = (int)std::min<int64_t>(G, q.nitems);
   q.args = new (std::nothrow) QArgs();
   if (!q.args) return MCFFT_ALLOC_FAILED;
+  q.stall = std::getenv("MCFFT_INJECT_STALL") != nullptr;
   q.on = true;
   return MCFFT_SUCCESS;
 }
@@ -880,7 +887,7 @@ mcfftResult exec_queue(mcfftPlan p, const void* in, void* out, int dir, cudaStre
                     &Q))
       return MCFFT_CUDA_ERROR;
     Q.wait_base = q.wait_base[i];
-    Q.wait_count = ps.wait_count;
+    Q.wait_count = q.stall && Q.wait_base >= 0 ? INT32_MAX : ps.wait_count;
     Q.sig_base = q.sig_base[i];
     Q.sig_mul = ps.sig_mul;
     Q.sig_div = ps.sig_div;

@@ -40,14 +40,25 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
   return ok != 0;
 }
 
-// Bounded wait on an mbarrier phase.  Returns false if `limit` polls pass
-// without the phase completing (the caller records an error and leaves).
+// Low 32 bits of the GPU's global nanosecond timer (independent of the SM
+// clock).  They wrap every 4.29 s, so a difference of two readings taken
+// less than that apart is exact in unsigned arithmetic.
+__device__ __forceinline__ uint32_t globaltimer_ns() {
+  uint32_t t;
+  asm volatile("mov.u32 %0, %%globaltimer_lo;" : "=r"(t));
+  return t;
+}
+
+// Bounded wait on an mbarrier phase.  Returns false if the phase has not
+// completed `limit_ns` (< 2^32) nanoseconds of global time after the wait
+// began (the caller records an error and leaves).
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity,
-                                                  uint32_t limit) {
-  for (uint32_t i = 0; i < limit; ++i) {
-    if (mbar_try_wait(bar, parity)) return true;
+                                                  uint32_t limit_ns) {
+  const uint32_t t0 = globaltimer_ns();
+  while (!mbar_try_wait(bar, parity)) {
+    if (globaltimer_ns() - t0 > limit_ns) return false;
   }
-  return false;
+  return true;
 }
 
 __device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
