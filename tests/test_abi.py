@@ -42,6 +42,14 @@ def test_invalid_arguments_rejected():
     assert L.mcfftExec(None, None, None, mc.FORWARD, None) == mc.INVALID_PLAN
     assert L.mcfftPlanDestroy(None) == mc.INVALID_PLAN
     assert L.mcfftPlanGetInfo(None, None) == mc.INVALID_PLAN
+    # empty batches, impossible dimensionality and negative offsets too
+    assert L.mcfftPlanCreate1d(ctypes.byref(h), 256, 0, mc.PREC_FP16, 0) == mc.INVALID_VALUE
+    assert L.mcfftPlanCreate2d(ctypes.byref(h), 64, 64, -1, mc.PREC_SPLIT, 0) == mc.INVALID_VALUE
+    for ndim, batch, ioff, ooff in ((0, 1, 0, 0), (4, 1, 0, 0), (1, 1, -16, 0), (1, 1, 0, -16)):
+        d = mc.Desc(ndim, (ctypes.c_int64 * 3)(256, 1, 1), batch, ioff, ooff)
+        assert L.mcfftPlanCreateBatch(ctypes.byref(h), ctypes.byref(d), 1, mc.PREC_FP16, 0) \
+            == mc.INVALID_VALUE, (ndim, batch, ioff, ooff)
+    assert not h.value  # nothing was created
 
 
 def test_no_device_is_an_error_not_a_fallback():
