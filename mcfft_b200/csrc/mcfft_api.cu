@@ -36,6 +36,7 @@
 #include "../../include/mcfft.h"
 #include "mcfft_internal.h"
 #include "queue.h"
+#include "queue_order.h"
 #include "tile_pass.h"
 
 namespace mcfft {
@@ -784,12 +785,13 @@ mcfftResult build_group(mcfftPlan p, int ndim, const int64_t* dims, int64_t batc
 // parameter block; otherwise the plan launches pass by pass (one transform
 // shape is faster that way: each pass kernel keeps its tables in its
 // parameter block).
-// Queue order: per transform group, the first pass's tiles in chunks of
-// QC (sixteen) per CTA, each later pass's tile for key k once the previous
-// pass's tiles for keys up to k + W are queued (W ~ QC tiles per CTA of lag), so
-// every dependency points backwards, a CTA runs several tiles of one pass
-// in a row (its tables stay in shared memory), and the intermediate is read
-// back while it is in L2.
+// Queue order (queue_order.h): first passes in chunks of QC (sixteen) tiles
+// per CTA, group after group; after each chunk, every later-pass tile whose
+// key was completed at least QC tiles per CTA earlier, across all groups.
+// Every dependency points backwards, a CTA runs several tiles of one pass in
+// a row (its tables stay in shared memory), and the tail of one group's
+// later pass runs beside the next group's first pass instead of waiting on
+// the tiles queued just before it.
 mcfftResult build_queue(mcfftPlan p) {
   bool want = p->ngroups > 1;
   if (const char* e = std::getenv("MCFFT_QUEUE")) want = std::atoi(e) != 0;
@@ -815,41 +817,25 @@ mcfftResult build_queue(mcfftPlan p) {
       q.sig_base[i - 1] = (int)nc;
       nc += p->passes[i].keys;
     }
-  std::vector<QItem> items;
   const int64_t G = maxg;
   // first-pass tiles per CTA queued at a time (a CTA reloads a pass's tables when its
   // consecutive items switch pass)
   int64_t QC = 16;
   if (const char* e = std::getenv("MCFFT_QUEUE_CHUNK")) QC = std::max<int64_t>(1, std::atoll(e));
-  for (size_t i = 0; i < np;) {
-    size_t j = i;
-    while (j < np && p->passes[j].grp == p->passes[i].grp) ++j;
-    const int nl = (int)(j - i);
-    std::vector<int64_t> tot(nl), em(nl, 0), W(nl, 0);
-    for (int l = 0; l < nl; ++l) tot[l] = p->passes[i + l].tp.args.ntiles;
-    for (int l = 1; l < nl; ++l) {
-      const Pass& P = p->passes[i + l - 1];
-      W[l] = std::max<int64_t>(1, (QC * G * P.sig_mul + P.sig_div - 1) / P.sig_div);
-    }
-    for (bool left = true; left;) {
-      for (int64_t c = 0; c < QC * G && em[0] < tot[0]; ++c)
-        items.push_back({(uint32_t)i, (uint32_t)em[0]++});
-      for (int l = 1; l < nl; ++l) {
-        const Pass& P = p->passes[i + l - 1];
-        const Pass& Q = p->passes[i + l];
-        while (em[l] < tot[l]) {
-          const int64_t key = em[l] / Q.tp.args.col_blocks;
-          const bool all = em[l - 1] == tot[l - 1];
-          const int64_t done = em[l - 1] * P.sig_mul / P.sig_div;
-          if (!all && done < key + 1 + W[l]) break;
-          items.push_back({(uint32_t)(i + l), (uint32_t)em[l]++});
-        }
-      }
-      left = false;
-      for (int l = 0; l < nl; ++l) left |= em[l] < tot[l];
-    }
-    i = j;
+  std::vector<QOrderPass> qo(np);
+  for (size_t i = 0; i < np; ++i) {
+    const Pass& ps = p->passes[i];
+    qo[i].ntiles = ps.tp.args.ntiles;
+    qo[i].col_blocks = ps.tp.args.col_blocks;
+    qo[i].sig_mul = ps.sig_mul;
+    qo[i].sig_div = ps.sig_div;
+    qo[i].keys = ps.level > 0 ? ps.keys : 0;
+    qo[i].grp = ps.grp;
   }
+  const std::vector<QOrderItem> order = queue_order(qo, G, QC);
+  if (order.empty()) return MCFFT_SUCCESS;  // no consistent order: pass by pass
+  std::vector<QItem> items(order.size());
+  for (size_t i = 0; i < order.size(); ++i) items[i] = {order[i].pass, order[i].tile};
   mcfftResult r = plan_alloc(p, &q.items, items.size() * sizeof(QItem));
   if (!r) r = plan_alloc(p, &q.counters, (size_t)std::max<int64_t>(nc, 1) * sizeof(int));
   if (r) return r;
