@@ -16,9 +16,12 @@ namespace mcfft {
 
 namespace {
 
-// Two tile sizes: 16K points with 16 consumer warps at one CTA per SM, and
-// 8K points with 8 consumer warps at two CTAs per SM (the two CTAs' phases
-// -- prologue, MMA wait, epilogue -- interleave on the SM).
+// Two tile sizes, both with 16 consumer warps at one CTA per SM: 16K points
+// (the default), and 8K points, half the work per thread and so about half
+// the latency per tile, which the plan-time tuner takes where a pass has
+// too few tiles to fill the SMs (small batches).  8K tiles need at least
+// four columns (L <= 2048).  These 8K routines are the ones the batch
+// kernel runs for a pass tuned to 8K.
 template <int L, int R, bool PT, int TP, int NCW>
 TileKernel make_f16() {
   constexpr int C = TP / L;
@@ -38,7 +41,7 @@ TileKernel make_f16() {
 const std::vector<TileKernel>& registry() {
   static const std::vector<TileKernel> v = {
       MCFFT_TILE_VARIANTS(false, 16384, 16), MCFFT_TILE_VARIANTS(true, 16384, 16),
-      MCFFT_TILE_VARIANTS(false, 8192, 8), MCFFT_TILE_VARIANTS(true, 8192, 8)};
+      MCFFT_TILE_VARIANTS(false, 8192, 16), MCFFT_TILE_VARIANTS(true, 8192, 16)};
   return v;
 }
 

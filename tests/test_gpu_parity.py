@@ -142,3 +142,21 @@ def test_partial_tile_batch():
     ref = oracle.fft1d(rounded(x, True)) * 2.0 ** sl
     rel, _ = compare(y, ref)
     assert rel < PLAIN_TOL, rel
+
+
+@pytest.mark.parametrize("shape,batch", [((32,), 512), ((64,), 256), ((128,), 128), ((256,), 67),
+                                         ((512,), 32), ((1024,), 16), ((2048,), 8), ((2048,), 5),
+                                         ((1 << 20,), 1), ((512, 512), 1), ((64, 64, 64), 1)])
+def test_plain_8k_tiles(shape, batch, monkeypatch):
+    """The 8K-point tile variants, which the plan-time tuner takes where they
+    are faster, forced for every pass (first choice 8K, tuning off).  Every
+    pass here has an 8K layout (at least four columns per tile; L = 4096
+    has none and always runs 16K tiles)."""
+    monkeypatch.setenv("MCFFT_TILE_POINTS", "8192")
+    monkeypatch.setenv("MCFFT_AUTOTUNE", "0")
+    x = rand_complex((batch,) + shape, seed=len(shape) * 1000 + batch)
+    with mc.Plan(shape, batch, mc.PREC_FP16) as p:
+        y, sl = run(p, x, True)
+    ref = oracle.fftnd(rounded(x, True), shape) * 2.0 ** sl
+    rel, mx = compare(y, ref)
+    assert rel < PLAIN_TOL, (rel, mx)
