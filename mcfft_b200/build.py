@@ -26,8 +26,8 @@ FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O2",
 SOURCES = ["tables.cu", "pass_kernels.cu", "tile_pass.cu", "tile_split.cu", "queue.cu",
            "queue_split.cu", "layout.cpp", "mcfft_api.cu", "noalloc.cu"]
 HEADERS = ["sm100_ptx.cuh", "tail_layout.h", "fft_pass.cuh", "fft_pass_split.cuh", "fft_tile.cuh",
-           "fft_tile_split.cuh", "fft_queue.cuh", "queue.h", "queue_order.h", "tile_pass.h", "layout.h",
-           "mcfft_internal.h"]
+           "fft_tile_split.cuh", "fft_queue.cuh", "queue.h", "queue_order.h", "host_schedule.h",
+           "tile_pass.h", "layout.h", "mcfft_internal.h"]
 
 
 def _stale(target: str, deps) -> bool:

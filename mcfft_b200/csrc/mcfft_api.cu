@@ -36,6 +36,7 @@
 #include "../../include/mcfft.h"
 #include "mcfft_internal.h"
 #include "queue.h"
+#include "host_schedule.h"
 #include "queue_order.h"
 #include "tile_pass.h"
 
@@ -1010,33 +1011,10 @@ mcfftResult exec_launches(mcfftPlan p, const void* in, void* out, int dir, cudaS
   return MCFFT_SUCCESS;
 }
 
-// Chunk schedule of mcfftExecHost.  A single-shape plan (one descriptor,
-// no offsets) is cut into runs of whole transforms: lengths 1, 2, 4, ..
-// rising to B (the largest power of two with B transforms in at most
-// MCFFT_HOST_CHUNK_BYTES of input, default 32 MiB), runs of B, the rest in
-// powers of two, and the rising lengths again in reverse.  Short first and
-// last chunks shorten the time only one copy direction is busy (the first
-// copy in, the last copy out); long middle chunks keep the per-chunk cost
-// small.  Anything else is one chunk run by the plan itself.
-std::vector<int64_t> host_schedule(int64_t batch, int64_t big) {
-  std::vector<int64_t> head, mid;
-  int64_t rem = batch;
-  for (int64_t s = 1; s < big && rem >= 2 * s; s *= 2) {
-    head.push_back(s);
-    rem -= 2 * s;
-  }
-  for (; rem >= big; rem -= big) mid.push_back(big);
-  for (int64_t s = big; s >= 1; s /= 2)
-    if (rem >= s) {
-      mid.push_back(s);
-      rem -= s;
-    }
-  std::vector<int64_t> out = head;
-  out.insert(out.end(), mid.begin(), mid.end());
-  out.insert(out.end(), head.rbegin(), head.rend());
-  return out;
-}
-
+// Chunks and device buffers of mcfftExecHost.  A single-shape plan (one
+// descriptor, no offsets) follows the chunk schedule of host_schedule.h,
+// with one plan per chunk length; anything else is one chunk run by the
+// plan itself.
 mcfftResult host_pipe_setup(mcfftPlan p) {
   auto& h = p->host;
   const mcfftDesc& d = p->desc0;
@@ -1047,8 +1025,7 @@ mcfftResult host_pipe_setup(mcfftPlan p) {
     if (const char* e = std::getenv("MCFFT_HOST_CHUNK_BYTES")) target = std::max<int64_t>(1, std::atoll(e));
     h.in_per = (size_t)(p->info.in_bytes / d.batch);
     h.out_per = (size_t)(p->info.out_bytes / d.batch);
-    int64_t big = 1;
-    while (2 * big <= d.batch && 2 * big * (int64_t)h.in_per <= target) big *= 2;
+    const int64_t big = host_chunk_big(d.batch, (int64_t)h.in_per, target);
     int64_t first = 0;
     for (int64_t c : host_schedule(d.batch, big)) {
       mcfftPlan x = nullptr;
