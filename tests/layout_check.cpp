@@ -5,7 +5,8 @@
 // that the tables are consistent -- every A-operand slot of stage 0 is
 // written exactly once by the prologue, every staging slot is read once,
 // and the column items' twiddle rows land on the physical rows the folded
-// table stores them at, and that paired row items share their rows.
+// table stores them at, that paired row items share their rows, and that
+// every stage's epilogue stores tile their destination buffer.
 #include <cstdio>
 #include <cstdlib>
 #include <set>
@@ -67,5 +68,26 @@ int main(int argc, char** argv) {
     for (int it = 0; it < pl.items / 2; ++it)
       ok_tabs &= pl.item_tab[2 * it + 1] == pl.item_tab[2 * (it + pl.items / 2) + 1];
   std::printf("tables_consistent %d\n", ok_tabs ? 1 : 0);
+  // epilogue: in every stage the 16 stores of each row (4-byte FP16
+  // complex into the next stage's operand; after the last stage oe-byte
+  // elements into the output staging) are aligned, inside the buffer, and
+  // together write each of its L C slots exactly once
+  bool ok_epi = (int)pl.epi_tab.size() == pl.NST * pl.NROWS && (int)pl.kofs.size() == pl.NST * 16 &&
+                pl.NROWS * 16 == L * C;
+  for (int s = 0; s < pl.NST && ok_epi; ++s) {
+    const uint32_t eb = s == pl.NST - 1 ? (uint32_t)oe : 4u;
+    const uint32_t nslots = (uint32_t)(L * C);
+    std::set<uint32_t> slots;
+    for (int r = 0; r < pl.NROWS; ++r) {
+      const uint32_t dst = (pl.epi_tab[(size_t)s * pl.NROWS + r] & 0xFFFFu) << 2;
+      for (int k = 0; k < 16; ++k) {
+        const uint32_t o = dst ^ pl.kofs[(size_t)s * 16 + k];
+        ok_epi &= o % eb == 0 && o / eb < nslots;
+        ok_epi &= slots.insert(o / eb).second;
+      }
+    }
+    ok_epi &= slots.size() == nslots;
+  }
+  std::printf("epilogue_consistent %d\n", ok_epi ? 1 : 0);
   return 0;
 }

@@ -49,6 +49,7 @@ def run(exe, L, R, C, ik, ok):
 def test_layout_conflicts_and_tables(checker, L, R, C, ik, ok):
     out = run(checker, L, R, C, ik, ok)
     assert out["tables_consistent"] == "1"
+    assert out["epilogue_consistent"] == "1"
     assert float(out["epilogue_excess"]) == pytest.approx(0.0, abs=1e-9)
     pro = float(out["prologue_excess"])
     if (ik == "col" and L == 4096) or (ik == "row" and L in (64, 128, 4096)):
@@ -84,8 +85,25 @@ def test_split_layouts(checker, L, R, C, ik, ok, ie):
     assert r.returncode == 0, r.stdout + r.stderr
     out = dict(line.split(None, 1) for line in r.stdout.splitlines())
     assert out["tables_consistent"] == "1"
+    assert out["epilogue_consistent"] == "1"
     assert float(out["epilogue_excess"]) == pytest.approx(0.0, abs=1e-9)
     pro = float(out["prologue_excess"])
     assert pro <= 1.5 + 1e-9
     if L == 1024 or L == 512:
         assert pro == pytest.approx(0.0, abs=1e-9)
+
+
+PLAIN_8K_SHAPES = [  # L, R, C (8K-point tiles of the plain form, and L = 32 at 16K)
+    (32, 2, 256), (64, 4, 128), (128, 8, 64), (256, 1, 32), (512, 2, 16), (1024, 4, 8),
+    (2048, 8, 4), (32, 2, 512),
+]
+
+
+@pytest.mark.parametrize("L,R,C", PLAIN_8K_SHAPES)
+@pytest.mark.parametrize("ik,ok", [("col", "col"), ("row", "col"), ("row", "row")])
+def test_plain_8k_layouts_consistent(checker, L, R, C, ik, ok):
+    """Every table the plain 8K-point tile kernels read: prologue loads and
+    stores once per slot, epilogue stores tiling each stage's buffer."""
+    out = run(checker, L, R, C, ik, ok)
+    assert out["tables_consistent"] == "1"
+    assert out["epilogue_consistent"] == "1"
