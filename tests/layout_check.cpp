@@ -78,7 +78,14 @@ int main(int argc, char** argv) {
     const uint32_t eb = s == pl.NST - 1 ? (uint32_t)oe : 4u;
     const uint32_t nslots = (uint32_t)(L * C);
     std::set<uint32_t> slots;
+    // the row's aux word: a stage-twiddle row of stage s (the kernel reads
+    // row stage_tw_row0(s) + aux of its table, (L / R) / 16^(s+1) rows per
+    // stage), or on the last stage v C + c (four-step twiddle of vector v,
+    // column c)
+    const uint32_t naux = s == pl.NST - 1 ? (uint32_t)(pl.NV * C)
+                                          : (uint32_t)(((L / R) >> (4 * s)) / 16);
     for (int r = 0; r < pl.NROWS; ++r) {
+      ok_epi &= (pl.epi_tab[(size_t)s * pl.NROWS + r] >> 16) < naux;
       const uint32_t dst = (pl.epi_tab[(size_t)s * pl.NROWS + r] & 0xFFFFu) << 2;
       for (int k = 0; k < 16; ++k) {
         const uint32_t o = dst ^ pl.kofs[(size_t)s * 16 + k];
