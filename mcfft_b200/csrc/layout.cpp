@@ -456,7 +456,12 @@ bool build(PassLayout* pl, int L, int R, int C, Kind in_kind, Kind out_kind, int
   for (int t = L / R; t > 1; t >>= 4) ++nst;
   p.NST = nst;
   if ((1 << (4 * nst)) * R != L || nst < 1) { *err = "L is not 16^a * R"; return false; }
-  if (C < 4 || (C & (C - 1))) { *err = "C must be a power of two >= 4"; return false; }
+  // Column staging puts min(C, 128 / elem) columns innermost in its TMA box,
+  // which must span 16 bytes: C >= 4.  Row staging's innermost box
+  // dimension is points (128 bytes), so a row-in / row-out pass also takes
+  // two columns (L = 4096 in 8K-point tiles).
+  const int cmin = in_kind == ROW && out_kind == ROW ? 2 : 4;
+  if (C < cmin || (C & (C - 1))) { *err = "C must be a power of two >= 4 (>= 2 for row passes)"; return false; }
   if (in_kind == COL && (ncols % std::min(C, 128 / in_elem))) { *err = "ncols"; return false; }
   if (out_kind == COL && (ncols % std::min(C, 128 / out_elem))) { *err = "ncols"; return false; }
   p.in = make_staging(in_kind, L, C, in_elem, in_sp, in_sc, in_so, ncols, nouter);

@@ -121,6 +121,9 @@ struct mcfftPlan_st {
   mcfftPlanInfo info{};
   mcfft::Queue q;
   int ngroups = 0;
+  // The plan is meant for the batch queue (several transform groups, or
+  // MCFFT_QUEUE=1): its passes take only tile shapes the batch kernel holds.
+  bool queue_planned = false;
   // Executable graphs of recent execs, keyed by (in, out, direction): an
   // exec repeated on the same buffers replays its captured launches.
   struct GraphEntry {
@@ -306,6 +309,9 @@ mcfftResult add_tile_pass(mcfftPlan p, const PassSpec& s, int only_tile_points =
         find_tile_kernel((int)s.L, s.posttw, p->split, order[oi], s.in_f16 != 0);
     if (!cand) continue;
     if (!p->split && (in_elem != 4 || out_elem != 4)) continue;
+    // a plan meant for the batch queue takes only tile shapes the batch
+    // kernel holds (not L = 4096 in 8K-point tiles)
+    if (p->queue_planned && queue_variant(*cand) < 0) continue;
     std::string err;
     if (!tile_layout(&tp.lay, cand->L, cand->R, cand->C, ik, ok, in_elem, out_elem, s.in_sp,
                      s.in_sc, s.in_so, s.out_sp, s.out_sc, s.out_so, s.ncols, s.nouter, &err))
@@ -1151,17 +1157,25 @@ mcfftResult mcfftPlanCreateBatch(mcfftPlan* plan, const mcfftDesc* descs, int co
     for (int k = 0; k < d.ndim; ++k) t *= d.dims[k];
     return t;
   };
+  // group boundaries: i starts a group unless it continues the previous one
+  auto continues = [&](int i, const mcfftDesc& g) {
+    const mcfftDesc& d = descs[i];
+    bool same = d.ndim == g.ndim;
+    for (int k = 0; k < g.ndim && same; ++k) same = d.dims[k] == g.dims[k];
+    const int64_t len = g.batch * points(g);
+    return same && d.in_offset == g.in_offset + len && d.out_offset == g.out_offset + len;
+  };
+  int ngroups = 0;
+  for (int i = 0; i < count; ++ngroups) {
+    mcfftDesc g = descs[i];
+    for (++i; i < count && continues(i, g); ++i) g.batch += descs[i].batch;
+  }
+  p->queue_planned = ngroups > 1;
+  if (const char* e = std::getenv("MCFFT_QUEUE")) p->queue_planned = std::atoi(e) != 0;
   for (int i = 0; i < count && !r;) {
     mcfftDesc g = descs[i];
     int j = i + 1;
-    for (; j < count; ++j) {
-      const mcfftDesc& d = descs[j];
-      bool same = d.ndim == g.ndim;
-      for (int k = 0; k < g.ndim && same; ++k) same = d.dims[k] == g.dims[k];
-      const int64_t len = g.batch * points(g);
-      if (!same || d.in_offset != g.in_offset + len || d.out_offset != g.out_offset + len) break;
-      g.batch += d.batch;
-    }
+    for (; j < count && continues(j, g); ++j) g.batch += descs[j].batch;
     int sl = 0;
     r = build_group(p, g.ndim, g.dims, g.batch, g.in_offset, g.out_offset, &sl);
     elements += g.batch * points(g);

@@ -120,6 +120,15 @@ bool tile_layout(layout::PassLayout* out, int L, int R, int C, layout::Kind ik, 
   if (!layout::build(out, L, R, C, ik, ok, in_elem, out_elem, isp, isc, iso, osp, osc, oso, ncols,
                      nouter, err))
     return false;
+  // The kernels size their table reads at compile time (TileShape): items,
+  // epilogue rows and stages must be exactly what the layout holds.
+  const int items = R == 1 ? L * C / 16 : L * C / (4 * R);
+  if (out->items != items || out->NROWS != L / 16 * C ||
+      (int)out->item_tab.size() != 2 * items ||
+      out->epi_tab.size() != (size_t)out->NST * out->NROWS || out->kofs.size() != (size_t)out->NST * 16) {
+    *err = "layout tables do not match the kernel's tile shape";
+    return false;
+  }
   std::lock_guard<std::mutex> lk(g_lay_mu);
   g_lay_cache[key] = *out;
   return true;

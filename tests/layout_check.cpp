@@ -95,6 +95,9 @@ int main(int argc, char** argv) {
     }
     ok_epi &= slots.size() == nslots;
   }
+  // the kernel's compile-time table sizes (TileShape): items, rows, stages
+  const int items = R == 1 ? L * C / 16 : L * C / (4 * R);
+  ok_epi &= pl.items == items && (int)pl.item_tab.size() == 2 * items && pl.NROWS == L / 16 * C;
   std::printf("epilogue_consistent %d\n", ok_epi ? 1 : 0);
   return 0;
 }

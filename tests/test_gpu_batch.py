@@ -111,6 +111,18 @@ def test_queue_forced_single_shape(shape, batch, monkeypatch):
     assert _check_each(descs, xr, y, True) < PLAIN_TOL
 
 
+def test_uneven_batch_8k_tiles_stays_one_launch(monkeypatch):
+    # 8K-point tiles forced: every pass the batch kernel holds in 8K takes
+    # it (the batch kernel's 16-warp 8K routines); L = 4096 keeps 16K tiles,
+    # the only shape the batch kernel holds for it, so the plan stays one launch
+    monkeypatch.setenv("MCFFT_TILE_POINTS", "8192")
+    monkeypatch.setenv("MCFFT_AUTOTUNE", "0")
+    descs, total = _layout(SHAPES, 0)
+    xr, y, info = _run_batch(descs, total, mc.PREC_FP16, seed=9)
+    assert info.launches == 1, info.launches
+    assert _check_each(descs, xr, y, True) < PLAIN_TOL
+
+
 def test_queue_repeated_exec_and_inverse():
     # counters are reset per exec; the inverse direction uses the conjugate tables
     descs, total = _layout(SHAPES[:6], 0)

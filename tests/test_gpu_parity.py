@@ -146,12 +146,13 @@ def test_partial_tile_batch():
 
 @pytest.mark.parametrize("shape,batch", [((32,), 512), ((64,), 256), ((128,), 128), ((256,), 67),
                                          ((512,), 32), ((1024,), 16), ((2048,), 8), ((2048,), 5),
-                                         ((1 << 20,), 1), ((512, 512), 1), ((64, 64, 64), 1)])
+                                         ((4096,), 8), ((4096,), 3), ((1 << 20,), 1),
+                                         ((512, 512), 1), ((64, 64, 64), 1)])
 def test_plain_8k_tiles(shape, batch, monkeypatch):
     """The 8K-point tile variants, which the plan-time tuner takes where they
     are faster, forced for every pass (first choice 8K, tuning off).  Every
-    pass here has an 8K layout (at least four columns per tile; L = 4096
-    has none and always runs 16K tiles)."""
+    pass here has an 8K layout; L = 4096 row passes take two columns per
+    tile (batch 3: the last column block half empty)."""
     monkeypatch.setenv("MCFFT_TILE_POINTS", "8192")
     monkeypatch.setenv("MCFFT_AUTOTUNE", "0")
     x = rand_complex((batch,) + shape, seed=len(shape) * 1000 + batch)

@@ -99,6 +99,19 @@ PLAIN_8K_SHAPES = [  # L, R, C (8K-point tiles of the plain form, and L = 32 at 
 ]
 
 
+def test_two_column_row_layout(checker):
+    """L = 4096 in 8K-point tiles: two columns per tile, allowed for row-in /
+    row-out passes only (column staging needs four columns across its
+    16-byte TMA box)."""
+    out = run(checker, 4096, 1, 2, "row", "row")
+    assert out["tables_consistent"] == "1"
+    assert out["epilogue_consistent"] == "1"
+    for ik, ok in (("col", "col"), ("row", "col")):
+        r = subprocess.run([checker, "4096", "1", "2", ik, ok], capture_output=True, text=True,
+                           timeout=120)
+        assert r.returncode == 1 and r.stdout.startswith("error"), r.stdout
+
+
 @pytest.mark.parametrize("L,R,C", PLAIN_8K_SHAPES)
 @pytest.mark.parametrize("ik,ok", [("col", "col"), ("row", "col"), ("row", "row")])
 def test_plain_8k_layouts_consistent(checker, L, R, C, ik, ok):
