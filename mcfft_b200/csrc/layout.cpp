@@ -461,7 +461,10 @@ bool build(PassLayout* pl, int L, int R, int C, Kind in_kind, Kind out_kind, int
   // dimension is points (128 bytes), so a row-in / row-out pass also takes
   // two columns (L = 4096 in 8K-point tiles).
   const int cmin = in_kind == ROW && out_kind == ROW ? 2 : 4;
-  if (C < cmin || (C & (C - 1))) { *err = "C must be a power of two >= 4 (>= 2 for row passes)"; return false; }
+  if (C < cmin || (C & (C - 1))) {
+    *err = "C must be a power of two >= 4 (>= 2 for row passes)";
+    return false;
+  }
   if (in_kind == COL && (ncols % std::min(C, 128 / in_elem))) { *err = "ncols"; return false; }
   if (out_kind == COL && (ncols % std::min(C, 128 / out_elem))) { *err = "ncols"; return false; }
   p.in = make_staging(in_kind, L, C, in_elem, in_sp, in_sc, in_so, ncols, nouter);
