@@ -30,8 +30,9 @@
  *                     MCFFT_FLAG_INPUT_F16), FP32 out, unnormalised DFT
  *                     (scale_log2 = 0), like FFTW_FORWARD/FFTW_BACKWARD.
  *
- * Sizes: every dimension a power of two >= 16; 1D lengths up to 2^26 (two
- * passes above 8192); 2D/3D sides up to 8192.
+ * Sizes: every dimension a power of two >= 16; 1D lengths up to 2^26 (one
+ * pass up to 4096, split form 2048; a four-step pair of passes above);
+ * 2D/3D sides up to 8192 (one pass per axis).
  */
 #ifndef MCFFT_H_
 #define MCFFT_H_
