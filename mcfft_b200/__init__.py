@@ -162,12 +162,24 @@ class Plan:
 
     def exec(self, x, out=None, direction: int = FORWARD):
         """Run on torch CUDA tensors (complex32 for the FP16 forms, complex64
-        for FP32) on the current stream; returns `out`."""
+        for FP32) on the current stream; returns `out`.  Both tensors must be
+        contiguous and hold at least the plan's input / output bytes (the
+        kernels read and write the extents the plan describes)."""
         import torch
+        inf = self.info()
+
+        def need(t, nbytes, what):
+            if not (t.is_cuda and t.is_contiguous()):
+                raise ValueError(f"{what} must be a contiguous CUDA tensor")
+            have = t.numel() * t.element_size()
+            if have < nbytes:
+                raise ValueError(f"{what} holds {have} bytes; the plan needs {nbytes}")
+
+        need(x, inf.in_bytes, "x")
         if out is None:
             dt = torch.complex64 if self.precision == PREC_SPLIT else torch.complex32
-            n = self.info().elements
-            out = torch.empty(n, dtype=dt, device=x.device)
+            out = torch.empty(inf.elements, dtype=dt, device=x.device)
+        need(out, inf.out_bytes, "out")
         stream = torch.cuda.current_stream(x.device).cuda_stream
         self.exec_ptr(x.data_ptr(), out.data_ptr(), direction, stream)
         return out

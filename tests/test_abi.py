@@ -1,6 +1,7 @@
 """CPU tests of the C ABI boundary: the library loads, exports every symbol
-include/mcfft.h declares, reports errors without a device, and its host-side
-layout engine produces conflict-free, XOR-linear tables.  No GPU compute."""
+include/mcfft.h declares, reports errors without a device and refuses bad
+arguments before touching one; the Python binding checks its tensors
+before a launch.  No GPU compute."""
 import ctypes
 import os
 import re
@@ -67,3 +68,19 @@ def test_header_declares_compat_entry_points():
         src = open(os.path.join(ROOT, "include", h)).read()
         for fn in ("setup", "doit", "finalize", "generate_data"):
             assert re.search(r"\b%s\s*\(" % fn, src), (h, fn)
+
+
+def test_torch_exec_refuses_unusable_tensors():
+    """Plan.exec checks its tensors before any launch: a host tensor is
+    refused (the plan shell here has no device plan; info() is stubbed)."""
+    torch = pytest.importorskip("torch")
+    p = mc.Plan.__new__(mc.Plan)
+    p._h = ctypes.c_void_p()
+    p.precision = mc.PREC_FP16
+    inf = mc.PlanInfo()
+    inf.elements, inf.in_bytes, inf.out_bytes = 16, 64, 64
+    p.info = lambda: inf
+    with pytest.raises(ValueError, match="contiguous CUDA tensor"):
+        p.exec(torch.zeros(32, dtype=torch.float16))
+    with pytest.raises(ValueError, match="contiguous CUDA tensor"):
+        p.exec(torch.zeros(64, dtype=torch.float16)[::2])
