@@ -3,6 +3,7 @@
 // encoding and launch.
 #include <cstdio>
 #include <cstring>
+#include <deque>
 #include <map>
 #include <mutex>
 #include <string>
@@ -90,8 +91,13 @@ bool encode(CUtensorMap* map, const layout::Staging& s, const void* base) {
 }
 
 // Layouts are pure functions of their parameters; memoise them per process.
+// Layouts already built, by pass shape (the search takes up to seconds).
+// Bounded: past kLayoutCacheMax entries the oldest is dropped, so a process
+// that plans many batch sizes does not grow without limit.
+constexpr size_t kLayoutCacheMax = 256;
 std::mutex g_lay_mu;
 std::map<std::string, layout::PassLayout> g_lay_cache;
+std::deque<std::string> g_lay_order;  // insertion order of g_lay_cache's keys
 
 }  // namespace
 
@@ -130,7 +136,13 @@ bool tile_layout(layout::PassLayout* out, int L, int R, int C, layout::Kind ik, 
     return false;
   }
   std::lock_guard<std::mutex> lk(g_lay_mu);
-  g_lay_cache[key] = *out;
+  if (g_lay_cache.emplace(key, *out).second) {
+    g_lay_order.push_back(key);
+    while (g_lay_order.size() > kLayoutCacheMax) {
+      g_lay_cache.erase(g_lay_order.front());
+      g_lay_order.pop_front();
+    }
+  }
   return true;
 }
 
