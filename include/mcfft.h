@@ -157,10 +157,35 @@ MCFFT_API const char* mcfftGetErrorString(mcfftResult result);
  * n * batch FP16 complex values.  Limits: n a power of two in
  * [2^14, 2^22], n * batch <= 2^22 (16 MiB scratch); larger sizes return
  * MCFFT_UNSUPPORTED_SIZE or MCFFT_INVALID_VALUE.  The first call on a device
- * looks up the arrays' device addresses and should come before any stream
- * capture.  All calls share the arrays: calls that overlap on the GPU race. */
+ * looks up the arrays' device addresses (and creates one event and one
+ * stream) and should come before any stream capture.  All calls share the
+ * arrays: calls that overlap on the GPU race.  The tables are regenerated
+ * only when (n, direction) differs from the previous call's on the device.
+ * A device-side wait that ran out in an earlier call is reported by a later
+ * call, once the earlier one has completed, as MCFFT_DEVICE_TIMEOUT (that
+ * call does not transform; the condition is then cleared). */
 MCFFT_API mcfftResult mcfftExec1dNoAlloc(const void* in, void* out, int64_t n, int64_t batch,
                                          int direction, void* stream);
+
+/* Error norms of a result against an FP64 reference, reduced in FP64 on
+ * the GPU.  Replaces the host-side error reduction of the reference's
+ * accuracy harness (get_error, benchmark/accuracy_1d.cpp:26-56, and
+ * benchmark/accuracy_2d.cpp:26-56), which walks the whole result on the
+ * CPU.  `y`: device, complex FP16 (y_f16 = 1) or FP32 (y_f16 = 0)
+ * interleaved; `ref`: device, complex FP64 interleaved, same element count.
+ * The elements are cut into `nseg` segments [seg_off[i], seg_off[i + 1])
+ * (host array of nseg + 1 offsets, e.g. one per transform); y of segment i
+ * is scaled by 2^seg_scale_log2[i] first (host array, or NULL for no
+ * scaling; the plain form's output carries 2^scale_log2).  out (host,
+ * 5 * nseg doubles), per segment: sum |y - ref|^2, sum |ref|^2,
+ * max |y - ref| and max |ref| (over real and imaginary parts separately),
+ * and the reference harness's sum over real and
+ * imaginary components of min(1, |(y - ref) / ref|) (divide by the number
+ * of complex elements for its get_error value).  Allocates a small device
+ * block for its tables and synchronises `stream` before returning. */
+MCFFT_API mcfftResult mcfftErrorNorms(const void* y, int y_f16, const void* ref, int nseg,
+                                      const int64_t* seg_off, const int* seg_scale_log2,
+                                      double* out, void* stream);
 
 /* Autotuning records ("wisdom"; the reference has no tuner and no such
  * file).  Creating a plain-form plan times each pass's two tile shapes once

@@ -40,7 +40,7 @@ EXPORTS = (
     "mcfftPlanCreate1d", "mcfftPlanCreate2d", "mcfftPlanCreate3d", "mcfftPlanCreateBatch",
     "mcfftExec", "mcfftPlanCheckStatus", "mcfftPlanGetInfo", "mcfftPlanDestroy",
     "mcfftGetErrorString", "mcfftGetVersion", "mcfftExec1dNoAlloc", "mcfftExecHost",
-    "mcfftWisdomExport", "mcfftWisdomImport", "mcfftWisdomForget",
+    "mcfftWisdomExport", "mcfftWisdomImport", "mcfftWisdomForget", "mcfftErrorNorms",
 )
 
 
@@ -96,6 +96,9 @@ def lib() -> ctypes.CDLL:
         L.mcfftGetVersion.restype = ci
         L.mcfftExec1dNoAlloc.argtypes = [P, P, i64, i64, ci, P]
         L.mcfftExec1dNoAlloc.restype = ci
+        L.mcfftErrorNorms.argtypes = [P, ci, P, ci, ctypes.POINTER(i64), ctypes.POINTER(ci),
+                                      ctypes.POINTER(ctypes.c_double), P]
+        L.mcfftErrorNorms.restype = ci
         for name in ("mcfftPlanCreate1d", "mcfftPlanCreate2d", "mcfftPlanCreate3d",
                      "mcfftPlanCreateBatch", "mcfftExec", "mcfftExecHost", "mcfftPlanCheckStatus",
                      "mcfftPlanGetInfo", "mcfftPlanDestroy"):
@@ -140,6 +143,14 @@ class Plan:
         self.precision = precision
         self.flags = flags
         self.descs = descs
+        # plans live on the device current at creation (cudaGetDevice)
+        self.device_index = None
+        try:
+            import torch
+            if torch.cuda.is_available():
+                self.device_index = torch.cuda.current_device()
+        except ImportError:
+            pass
 
     @property
     def handle(self):
@@ -161,26 +172,40 @@ class Plan:
                                    direction, ctypes.c_void_p(stream)), "mcfftExecHost")
 
     def exec(self, x, out=None, direction: int = FORWARD):
-        """Run on torch CUDA tensors (complex32 for the FP16 forms, complex64
-        for FP32) on the current stream; returns `out`.  Both tensors must be
-        contiguous and hold at least the plan's input / output bytes (the
-        kernels read and write the extents the plan describes)."""
+        """Run on torch CUDA tensors on the current stream; returns `out`.
+        Element types: the input is complex32 (FP16) for the plain form and
+        for the split form with FLAG_INPUT_F16, complex64 (FP32) otherwise;
+        the output is complex32 for the plain form, complex64 for split.
+        Both tensors must be contiguous, on the plan's device, and hold at
+        least the plan's input / output bytes (the kernels read and write the
+        extents the plan describes)."""
         import torch
         inf = self.info()
+        split = self.precision == PREC_SPLIT
+        in_dt = torch.complex64 if split and not (self.flags & FLAG_INPUT_F16) else torch.complex32
+        out_dt = torch.complex64 if split else torch.complex32
+        dev = None
 
-        def need(t, nbytes, what):
+        def need(t, dtype, nbytes, what):
+            nonlocal dev
             if not (t.is_cuda and t.is_contiguous()):
                 raise ValueError(f"{what} must be a contiguous CUDA tensor")
+            if dev is None:
+                dev = torch.device("cuda", self.device_index if self.device_index is not None
+                                   else torch.cuda.current_device())
+            if t.dtype != dtype:
+                raise ValueError(f"{what} is {t.dtype}; this plan needs {dtype}")
+            if t.device != dev:
+                raise ValueError(f"{what} is on {t.device}; the plan was made on {dev}")
             have = t.numel() * t.element_size()
             if have < nbytes:
                 raise ValueError(f"{what} holds {have} bytes; the plan needs {nbytes}")
 
-        need(x, inf.in_bytes, "x")
+        need(x, in_dt, inf.in_bytes, "x")
         if out is None:
-            dt = torch.complex64 if self.precision == PREC_SPLIT else torch.complex32
-            out = torch.empty(inf.elements, dtype=dt, device=x.device)
-        need(out, inf.out_bytes, "out")
-        stream = torch.cuda.current_stream(x.device).cuda_stream
+            out = torch.empty(inf.elements, dtype=out_dt, device=dev)
+        need(out, out_dt, inf.out_bytes, "out")
+        stream = torch.cuda.current_stream(dev).cuda_stream
         self.exec_ptr(x.data_ptr(), out.data_ptr(), direction, stream)
         return out
 
@@ -211,6 +236,40 @@ def exec_1d_no_alloc(in_ptr: int, out_ptr: int, n: int, batch: int,
     device arrays inside the library; see include/mcfft.h)."""
     _check(lib().mcfftExec1dNoAlloc(ctypes.c_void_p(in_ptr), ctypes.c_void_p(out_ptr), n, batch,
                                     direction, ctypes.c_void_p(stream)), "mcfftExec1dNoAlloc")
+
+
+def error_norms(y_ptr: int, y_f16: bool, ref_ptr: int, seg_off, seg_scale_log2=None,
+                stream: int = 0):
+    """FP64 error norms on the GPU (see mcfftErrorNorms in include/mcfft.h).
+
+    y_ptr: device result (complex FP16 if y_f16, else complex FP32); ref_ptr:
+    device complex FP64 reference; seg_off: nseg + 1 element offsets;
+    seg_scale_log2: per-segment power-of-two scale of y (or None).  Returns
+    a list of per-segment dicts: rel_l2, max_rel (max |y - ref| / max |ref|)
+    and get_error (the reference harness's metric)."""
+    offs = [int(v) for v in seg_off]
+    nseg = len(offs) - 1
+    if nseg < 1:
+        raise ValueError("need at least one segment")
+    off_arr = (ctypes.c_int64 * len(offs))(*offs)
+    sc_arr = None
+    if seg_scale_log2 is not None:
+        sc = [int(v) for v in seg_scale_log2]
+        if len(sc) != nseg:
+            raise ValueError("one scale per segment")
+        sc_arr = (ctypes.c_int * nseg)(*sc)
+    out = (ctypes.c_double * (5 * nseg))()
+    _check(lib().mcfftErrorNorms(ctypes.c_void_p(y_ptr), int(bool(y_f16)), ctypes.c_void_p(ref_ptr),
+                                 nseg, off_arr, sc_arr, out, ctypes.c_void_p(stream)),
+           "mcfftErrorNorms")
+    res = []
+    for i in range(nseg):
+        e2, r2, emax, rmax, rel = out[5 * i: 5 * i + 5]
+        n = offs[i + 1] - offs[i]
+        res.append({"rel_l2": (e2 / r2) ** 0.5 if r2 > 0 else float("inf"),
+                    "max_rel": emax / rmax if rmax > 0 else float("inf"),
+                    "get_error": rel / n if n else 0.0})
+    return res
 
 
 def wisdom_export(path: str):

@@ -15,13 +15,21 @@
 // <= kNoAllocMaxPoints (4 Mi complex points, the 16 MiB scratch array).
 //
 // The first call on a device resolves the arrays' device addresses with
-// cudaGetSymbolAddress (with that device current); make that first call
-// before any stream capture.  Every call shares the arrays and leaves its
-// contents behind: two calls that overlap on the GPU (different streams,
-// different host threads) race on them.  The scratch needs no clearing --
-// pass 1 writes every element pass 2 reads.  The kernels' device status word
-// (bounded-wait timeouts) is also a file-scope array, reset at the start of
-// each call; this entry point does not read it back.
+// cudaGetSymbolAddress (with that device current) and creates one event and
+// one private stream; make that first call before any stream capture.  Every call shares the
+// arrays and leaves its contents behind: two calls that overlap on the GPU
+// (different streams, different host threads) race on them.  The scratch
+// needs no clearing -- pass 1 writes every element pass 2 reads.  The
+// twiddle tables and the DFT-16 matrix depend only on (n, direction): a call
+// whose (n, direction) equals the previous call's on that device reuses
+// them (the same overlap race covers this record).
+//
+// Device-side waits are bounded; a pass that gives up records a timeout in
+// a file-scope status word.  A call returns MCFFT_DEVICE_TIMEOUT, without
+// transforming, when it finds the status word of an earlier call on this
+// device set: the word is read back (4 bytes, on the private stream) only
+// once that earlier call's work has completed (an event query, so the call
+// never waits for it), and cleared.
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -52,6 +60,11 @@ struct DevAddrs {
   float2 *tw = nullptr, *tail = nullptr, *post_lo = nullptr, *post_hi = nullptr;
   uint4* bmat = nullptr;
   int* status = nullptr;
+  cudaEvent_t done = nullptr;  // recorded after each call's passes
+  cudaStream_t aux = nullptr;  // status read-back, never waits on the caller's work
+  bool pending = false;        // a call's status word has not been checked yet
+  int64_t tab_n = 0;           // (n, sign) whose tables are resident; 0: none
+  int tab_sign = 0;
 };
 constexpr int kMaxDevices = 64;
 DevAddrs g_addr[kMaxDevices];
@@ -76,10 +89,57 @@ mcfftResult setup_device(int dev, DevAddrs* out) {
     d.post_hi = static_cast<float2*>(p[4]);
     d.bmat = static_cast<uint4*>(p[5]);
     d.status = static_cast<int*>(p[6]);
+    if (!d.done && cudaEventCreateWithFlags(&d.done, cudaEventDisableTiming) != cudaSuccess) {
+      cudaGetLastError();
+      d.done = nullptr;
+      return MCFFT_CUDA_ERROR;
+    }
+    if (!d.aux && cudaStreamCreateWithFlags(&d.aux, cudaStreamNonBlocking) != cudaSuccess) {
+      cudaGetLastError();
+      d.aux = nullptr;
+      return MCFFT_CUDA_ERROR;
+    }
     d.ready = true;
   }
   *out = d;
   return MCFFT_SUCCESS;
+}
+
+// Status of the earlier call on this device, if its passes have finished:
+// MCFFT_DEVICE_TIMEOUT (and the word cleared) when one of them gave up.
+// A call still running is checked by a later call.
+mcfftResult check_earlier(int dev) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  DevAddrs& d = g_addr[dev];
+  if (!d.pending) return MCFFT_SUCCESS;
+  const cudaError_t q = cudaEventQuery(d.done);
+  if (q == cudaErrorNotReady) {
+    cudaGetLastError();
+    return MCFFT_SUCCESS;
+  }
+  if (q != cudaSuccess) {
+    cudaGetLastError();
+    return MCFFT_CUDA_ERROR;
+  }
+  d.pending = false;
+  int h = 0;
+  // The earlier call's work is complete and the private stream holds no
+  // other work, so neither this copy nor the clearing below waits for
+  // anything the caller enqueued.
+  if (cudaMemcpyFromSymbolAsync(&h, g_status, sizeof(int), 0, cudaMemcpyDeviceToHost, d.aux) !=
+          cudaSuccess ||
+      cudaStreamSynchronize(d.aux) != cudaSuccess) {
+    cudaGetLastError();
+    return MCFFT_CUDA_ERROR;
+  }
+  if (h == kStatusOk) return MCFFT_SUCCESS;
+  d.tab_n = 0;  // tables may be incomplete after an aborted call
+  if (cudaMemsetAsync(d.status, 0, sizeof(int), d.aux) != cudaSuccess ||
+      cudaStreamSynchronize(d.aux) != cudaSuccess) {
+    cudaGetLastError();
+    return MCFFT_CUDA_ERROR;
+  }
+  return h == kStatusTimeout ? MCFFT_DEVICE_TIMEOUT : MCFFT_INTERNAL_ERROR;
 }
 
 int ilog2i(int64_t x) {
@@ -116,7 +176,8 @@ extern "C" MCFFT_API mcfftResult mcfftExec1dNoAlloc(const void* in, void* out, i
   if (!in || !out || batch < 1) return MCFFT_INVALID_VALUE;
   if (direction != MCFFT_FORWARD && direction != MCFFT_INVERSE) return MCFFT_INVALID_VALUE;
   if (n < (int64_t(1) << 14) || n > (int64_t(1) << 22) || (n & (n - 1))) return MCFFT_UNSUPPORTED_SIZE;
-  if (n * batch > kNoAllocMaxPoints) return MCFFT_INVALID_VALUE;
+  // n * batch <= kNoAllocMaxPoints, written so that the product cannot overflow
+  if (batch > kNoAllocMaxPoints / n) return MCFFT_INVALID_VALUE;
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
     cudaGetLastError();
@@ -124,6 +185,8 @@ extern "C" MCFFT_API mcfftResult mcfftExec1dNoAlloc(const void* in, void* out, i
   }
   DevAddrs d;
   mcfftResult r = setup_device(dev, &d);
+  if (r != MCFFT_SUCCESS) return r;
+  r = check_earlier(dev);
   if (r != MCFFT_SUCCESS) return r;
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -140,16 +203,24 @@ extern "C" MCFFT_API mcfftResult mcfftExec1dNoAlloc(const void* in, void* out, i
   const PassKernel* k2 = pick_pass_kernel(n2, false, false, false, n1, 16384);
   if (!k1 || !k2 || k1->R != R1 || k2->R != R2) return MCFFT_UNSUPPORTED_SIZE;
 
-  cudaError_t e = cudaMemsetAsync(d.status, 0, sizeof(int), st);
-  if (e == cudaSuccess) e = gen_dft16_embedding(d.bmat, nullptr, sign, st);
   float2* tw2 = d.tw + 4096 + 256;
   float2* tail2 = d.tail + 2048;
-  if (e == cudaSuccess) e = pass_tables(n1, R1, d.tw, d.tail, sign, st);
-  if (e == cudaSuccess) e = pass_tables(n2, R2, tw2, tail2, sign, st);
   const int sh = lg / 2;
-  if (e == cudaSuccess)
-    e = gen_twiddle_table(d.post_lo, int64_t(1) << sh, 1, 0, 0, n, sign, 1.0, st);
-  if (e == cudaSuccess) e = gen_twiddle_table(d.post_hi, n >> sh, 1, 0, sh, n, sign, 1.0, st);
+  bool reuse = false;
+  {
+    std::lock_guard<std::mutex> lk(g_mu);
+    reuse = g_addr[dev].tab_n == n && g_addr[dev].tab_sign == sign;
+    g_addr[dev].tab_n = 0;  // set again once this call's tables are enqueued
+  }
+  cudaError_t e = cudaSuccess;
+  if (!reuse) {
+    e = gen_dft16_embedding(d.bmat, nullptr, sign, st);
+    if (e == cudaSuccess) e = pass_tables(n1, R1, d.tw, d.tail, sign, st);
+    if (e == cudaSuccess) e = pass_tables(n2, R2, tw2, tail2, sign, st);
+    if (e == cudaSuccess)
+      e = gen_twiddle_table(d.post_lo, int64_t(1) << sh, 1, 0, 0, n, sign, 1.0, st);
+    if (e == cudaSuccess) e = gen_twiddle_table(d.post_hi, n >> sh, 1, 0, sh, n, sign, 1.0, st);
+  }
   if (e != cudaSuccess) {
     cudaGetLastError();
     return MCFFT_CUDA_ERROR;
@@ -191,9 +262,14 @@ extern "C" MCFFT_API mcfftResult mcfftExec1dNoAlloc(const void* in, void* out, i
   const int g2 = (int)(a2.ntiles < 2 * sms ? a2.ntiles : 2 * sms);
   e = launch_pass(*k1, a1, g1, st);
   if (e == cudaSuccess) e = launch_pass(*k2, a2, g2, st);
+  if (e == cudaSuccess) e = cudaEventRecord(d.done, st);
   if (e != cudaSuccess) {
     cudaGetLastError();
     return MCFFT_CUDA_ERROR;
   }
+  std::lock_guard<std::mutex> lk(g_mu);
+  g_addr[dev].pending = true;
+  g_addr[dev].tab_n = n;
+  g_addr[dev].tab_sign = sign;
   return MCFFT_SUCCESS;
 }

@@ -6,6 +6,7 @@
 // the plain form); the planner picks among these.
 #include <cstdio>
 #include <mutex>
+#include <utility>
 #include <vector>
 
 #include "fft_pass.cuh"
@@ -94,17 +95,21 @@ const PassKernel* pick_pass_kernel(int L, bool colfast, bool posttw, bool split,
 }
 
 cudaError_t launch_pass(const PassKernel& k, const PassArgs& a, int grid, cudaStream_t st) {
+  // The shared-memory limit is a per-device attribute of the function: set
+  // it once for every (device, kernel) pair this process launches.
   static std::mutex mu;
-  static std::vector<const void*> configured;
+  static std::vector<std::pair<int, const void*>> configured;
   {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return cudaGetLastError();
     std::lock_guard<std::mutex> lock(mu);
     bool done = false;
-    for (auto f : configured) done |= (f == k.fn);
+    for (const auto& f : configured) done |= (f.first == dev && f.second == k.fn);
     if (!done) {
       cudaError_t e =
           cudaFuncSetAttribute(k.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, k.smem_bytes);
       if (e != cudaSuccess) return e;
-      configured.push_back(k.fn);
+      configured.push_back({dev, k.fn});
     }
   }
   void* args[] = {const_cast<PassArgs*>(&a)};

@@ -6,6 +6,7 @@
 #include <deque>
 #include <map>
 #include <mutex>
+#include <utility>
 #include <string>
 #include <vector>
 
@@ -167,17 +168,20 @@ cudaError_t launch_tile_pass(const TilePass& tp, const void* in, void* out, int 
   a.bmat = tp.bmat[dir];
   a.bmat_lo = tp.bmat_lo[dir];
   a.inverse = dir;
+  // The shared-memory limit is a per-device attribute of the function.
   static std::mutex mu;
-  static std::vector<const void*> configured;
+  static std::vector<std::pair<int, const void*>> configured;
   {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return cudaGetLastError();
     std::lock_guard<std::mutex> lock(mu);
     bool done = false;
-    for (auto f : configured) done |= (f == tp.k->fn);
+    for (const auto& f : configured) done |= (f.first == dev && f.second == tp.k->fn);
     if (!done) {
       cudaError_t e = cudaFuncSetAttribute(tp.k->fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            tp.k->smem_bytes);
       if (e != cudaSuccess) return e;
-      configured.push_back(tp.k->fn);
+      configured.push_back({dev, tp.k->fn});
     }
   }
   void* args[] = {&a};

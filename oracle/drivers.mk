@@ -4,7 +4,9 @@
 # infrastructure: outputs go to oracle/_ref/ (git-ignored; travels to the GPU
 # box).  Only builds where the reference is mounted.
 #   make -C oracle -f drivers.mk
-REF ?= /root/reference
+# The reference tree: MCFFT_REF_DIR, else the directory beside the repository.
+MCFFT_REF_DIR ?= $(abspath ../../reference)
+REF := $(MCFFT_REF_DIR)
 OUT := _ref
 CXX_ := /usr/bin/g++
 CC_ := /usr/bin/gcc

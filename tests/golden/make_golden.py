@@ -1,6 +1,6 @@
 """Extract the golden vectors that the reference's own files hold.
 
-Run here, where the reference is mounted:  python tests/golden/make_golden.py
+Run where the reference is mounted:  python tests/golden/make_golden.py [REF_DIR]
 Writes small fixtures next to this script; tests read only those.
 
 Sources (paths within the reference project):
@@ -20,8 +20,11 @@ import sys
 
 import numpy as np
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
 OUT = os.path.dirname(os.path.abspath(__file__))
+# The reference tree: the first argument, else $MCFFT_REF_DIR, else the
+# directory named `reference` beside this repository.
+REF = (sys.argv[1] if len(sys.argv) > 1 else os.environ.get("MCFFT_REF_DIR")
+       or os.path.join(os.path.dirname(os.path.dirname(os.path.dirname(OUT))), "reference"))
 KEEP = 16384  # doubles kept from each dump (8192 complex values)
 
 

@@ -77,6 +77,8 @@ def test_torch_exec_refuses_unusable_tensors():
     p = mc.Plan.__new__(mc.Plan)
     p._h = ctypes.c_void_p()
     p.precision = mc.PREC_FP16
+    p.flags = mc.FLAG_NONE
+    p.device_index = None
     inf = mc.PlanInfo()
     inf.elements, inf.in_bytes, inf.out_bytes = 16, 64, 64
     p.info = lambda: inf
@@ -84,3 +86,19 @@ def test_torch_exec_refuses_unusable_tensors():
         p.exec(torch.zeros(32, dtype=torch.float16))
     with pytest.raises(ValueError, match="contiguous CUDA tensor"):
         p.exec(torch.zeros(64, dtype=torch.float16)[::2])
+
+
+def test_error_norms_refuses_bad_segments():
+    """mcfftErrorNorms checks its segment table before touching a device."""
+    L = mc.lib()
+    one = ctypes.c_void_p(256)
+    out = (ctypes.c_double * 10)()
+    offs = (ctypes.c_int64 * 3)(0, 8, 4)  # decreasing
+    assert L.mcfftErrorNorms(one, 1, one, 2, offs, None, out, None) == mc.INVALID_VALUE
+    offs = (ctypes.c_int64 * 2)(-4, 4)  # negative
+    assert L.mcfftErrorNorms(one, 1, one, 1, offs, None, out, None) == mc.INVALID_VALUE
+    offs = (ctypes.c_int64 * 2)(0, 4)
+    assert L.mcfftErrorNorms(one, 1, one, 0, offs, None, out, None) == mc.INVALID_VALUE
+    assert L.mcfftErrorNorms(None, 1, one, 1, offs, None, out, None) == mc.INVALID_VALUE
+    with pytest.raises(ValueError):
+        mc.error_norms(256, True, 256, [0])

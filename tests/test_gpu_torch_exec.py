@@ -1,6 +1,7 @@
 """Plan.exec on torch CUDA tensors: the transform matches the FP64 oracle
 (plain form, rel-L2 <= 1e-3), and tensors smaller than the plan's input or
-output extents are refused before any launch."""
+output extents, or of the wrong element type, are refused before any
+launch."""
 import pytest
 
 pytestmark = pytest.mark.gpu
@@ -29,3 +30,19 @@ def test_torch_exec_matches_oracle_and_checks_sizes():
             p.exec(xd[: n * batch // 2])
         with pytest.raises(ValueError, match="bytes"):
             p.exec(xd, out=torch.empty(16, dtype=torch.complex32, device="cuda"))
+        # an FP32 tensor has enough bytes for this FP16 plan but the wrong type
+        with pytest.raises(ValueError, match="needs"):
+            p.exec(torch.zeros(n * batch, dtype=torch.complex64, device="cuda"))
+        with pytest.raises(ValueError, match="needs"):
+            p.exec(xd, out=torch.empty(n * batch, dtype=torch.complex64, device="cuda"))
+    with mc.Plan((n,), batch, mc.PREC_SPLIT) as p:
+        # the split form reads FP32 unless FLAG_INPUT_F16 and always writes FP32
+        with pytest.raises(ValueError, match="needs"):
+            p.exec(xd)
+        xf = to_device(x, False)
+        y = p.exec(xf)
+        torch.cuda.synchronize()
+        assert y.dtype == torch.complex64
+        ref = oracle.fft1d(rounded(x, False))
+        rel, _ = compare(from_device(y), ref)
+        assert rel < 2e-6, rel

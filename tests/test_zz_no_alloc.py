@@ -38,7 +38,10 @@ def _no_alloc(x, n, batch, direction):
     return from_device(out)
 
 
-@pytest.mark.parametrize("n,batch", [(1 << 16, 4), (1 << 20, 2), (1 << 15, 8)])
+# The last two fill the scratch array exactly: the largest n (its tables
+# fill the fixed arrays) and the smallest n with the largest batch.
+@pytest.mark.parametrize("n,batch", [(1 << 16, 4), (1 << 20, 2), (1 << 15, 8), (1 << 22, 1),
+                                     (1 << 14, 256)])
 def test_no_alloc_matches_plan_two_calls(n, batch):
     for call, direction in enumerate((mc.FORWARD, mc.INVERSE)):
         x = rand_complex((batch, n), seed=1000 + call)
@@ -59,4 +62,8 @@ def test_no_alloc_rejects_sizes_beyond_limits():
     assert L.mcfftExec1dNoAlloc(dummy, dummy, 1 << 12, 1, mc.FORWARD, None) == mc.UNSUPPORTED_SIZE
     assert L.mcfftExec1dNoAlloc(dummy, dummy, 3 << 14, 1, mc.FORWARD, None) == mc.UNSUPPORTED_SIZE
     assert L.mcfftExec1dNoAlloc(dummy, dummy, 1 << 20, 5, mc.FORWARD, None) == mc.INVALID_VALUE
+    # a batch whose product with n overflows 64 bits is refused too
+    assert L.mcfftExec1dNoAlloc(dummy, dummy, 1 << 22, 1 << 42, mc.FORWARD, None) == mc.INVALID_VALUE
+    assert L.mcfftExec1dNoAlloc(dummy, dummy, 1 << 14, (1 << 63) - 1, mc.FORWARD,
+                                None) == mc.INVALID_VALUE
     assert L.mcfftExec1dNoAlloc(None, dummy, 1 << 16, 1, mc.FORWARD, None) == mc.INVALID_VALUE
