@@ -262,7 +262,8 @@ def bench_uneven(args, torch, mc, stream, barrier, peak, gmax=lambda v: v, error
                      "ideal_hbm_ms": round(ideal_ms, 4), "vs_ideal": round(ms / ideal_ms, 3),
                      "launches_per_exec": info.launches, "passes": info.num_passes}
         if ref is not None:
-            scales = [-int(np.log2(np.prod(s))) if obytes == 4 else 0 for s in shapes]
+            # undo the plain form's output scale 2^-log2(N) of each transform
+            scales = [int(np.log2(np.prod(s))) if obytes == 4 else 0 for s in shapes]
             out[name]["error"] = device_errors(mc, torch, y, obytes == 4, ref, offs + [total],
                                                scales)
         del y
@@ -491,7 +492,7 @@ def accuracy_all(name, xc, dims, batch, plan, splan, s16, x, xs, torch, mc):
         xd16 = torch.from_numpy(interleaved(xin_c, True).copy()).cuda().view(torch.complex32)
         yp = run(plan, xd16, torch.complex32)
         out[tag + "plain"] = device_errors(mc, torch, yp, True, ref16, seg,
-                                           [plan.info().scale_log2] * batch)
+                                           [-plan.info().scale_log2] * batch)
         del yp
         if s16:
             ref_s, xd = ref16, xd16

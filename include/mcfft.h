@@ -30,9 +30,9 @@
  *                     MCFFT_FLAG_INPUT_F16), FP32 out, unnormalised DFT
  *                     (scale_log2 = 0), like FFTW_FORWARD/FFTW_BACKWARD.
  *
- * Sizes: every dimension a power of two >= 16; 1D lengths up to 2^26 (one
- * pass up to 4096, split form 2048; a four-step pair of passes above);
- * 2D/3D sides up to 8192 (one pass per axis).
+ * Sizes: every dimension a power of two >= 16; 1D lengths up to 2^27 (one
+ * pass up to 4096, split form 2048; a four-step pair of passes up to 2^26;
+ * three passes for 2^27); 2D/3D sides up to 8192 (one pass per axis).
  */
 #ifndef MCFFT_H_
 #define MCFFT_H_
@@ -176,7 +176,8 @@ MCFFT_API mcfftResult mcfftExec1dNoAlloc(const void* in, void* out, int64_t n, i
  * The elements are cut into `nseg` segments [seg_off[i], seg_off[i + 1])
  * (host array of nseg + 1 offsets, e.g. one per transform); y of segment i
  * is scaled by 2^seg_scale_log2[i] first (host array, or NULL for no
- * scaling; the plain form's output carries 2^scale_log2).  out (host,
+ * scaling; the plain form's output carries 2^scale_log2, so pass
+ * -scale_log2 to compare it with the unscaled DFT).  out (host,
  * 5 * nseg doubles), per segment: sum |y - ref|^2, sum |ref|^2,
  * max |y - ref| and max |ref| (over real and imaginary parts separately),
  * and the reference harness's sum over real and

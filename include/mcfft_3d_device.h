@@ -1,12 +1,31 @@
 /* mcfft_3d_device.h -- reference-compatible device-level entry points
- * (reference: include/mcfft_3d_device.h:37-38), implemented over the C ABI in mcfft.h by
- * libmcfft_3d.so.  No HIP or rocWMMA types.
+ * (reference: include/mcfft_3d_device.h:18-38), implemented over the C ABI in
+ * mcfft.h by libmcfft_3d.so.  No HIP or rocWMMA types.
+ *
+ * mcfftHandle has the reference's layout field for field
+ * (include/mcfft_3d_device.h:18-30 there), so that a caller compiled
+ * against the reference's header -- which passes the handle to mcfftExec
+ * by value -- runs unchanged against this library.  The fields keep their
+ * types' sizes; their use here:
+ *   Nx, Ny, N_batch           sides and transform count, as in the reference
+ *                             (3D: Ny holds ny * nz)
+ *   radices_x/_y, n_radices_  each side's radix factorisation 16^a * R (R
+ *                             first) where it fits three entries, else
+ *                             empty; informational
+ *   mergings                  zero
+ *   layer_0, layer_1          NULL (no per-layer kernel pointers)
+ *   F_real, F_imag            NULL (the DFT-16 matrix lives in the plan)
+ *   F_real_tmp                this library's plan (an mcfftPlan)
+ *   F_imag_tmp                its device FP32 work buffers *
+ * The reference's 3D files are its 2D files under another name (the same
+ * handle, nx and ny only); setup3d of include/mcfft_3d_utils.h takes the
+ * third side.
  *
  * Differences from the reference, all deliberate:
  *  - mcfftExec takes the data in natural order (the reference required the
- *    host digit reversal of source/mcfft_1d_utils.cpp:43-59 first);
+ *    host digit reversal of source/mcfft_2d_utils.cpp:45-53 first);
  *  - every size the core supports is accepted (the reference's table has
- *    ten 1D sizes and three 2D sides);
+ *    three 2D sides, and its 1024-side plan launches a missing kernel);
  *  - the plan owns device memory; mcfftDestroy releases it.
  */
 #ifndef MCFFT_3D_DEVICE_H_
@@ -17,8 +36,14 @@
 
 typedef struct {
   int Nx, Ny, N_batch;
-  mcfftPlan plan;   /* split-form plan (FP32 operands on the device) */
-  void* work;       /* device FP32 staging, 2 buffers */
+  int radices_x[3];
+  int radices_y[3];
+  int n_radices_x, n_radices_y;
+  int mergings[2];
+  void (*layer_0[3])(void*, MCTYPE*, MCTYPE*);
+  void (*layer_1[3])(int, void*, MCTYPE*, MCTYPE*);
+  MCTYPE *F_real, *F_imag;
+  MCTYPE *F_real_tmp, *F_imag_tmp;
 } mcfftHandle;
 
 /* In place on device FP64 interleaved complex data, forward transform,

@@ -24,7 +24,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O2",
          "-Xcompiler", "-fvisibility=hidden", "--expt-relaxed-constexpr"]
 SOURCES = ["tables.cu", "pass_kernels.cu", "tile_pass.cu", "tile_split.cu", "queue.cu",
-           "queue_split.cu", "layout.cpp", "mcfft_api.cu", "noalloc.cu", "norms.cu"]
+           "queue_split.cu", "fused.cu", "layout.cpp", "mcfft_api.cu", "noalloc.cu", "norms.cu"]
 HEADERS = ["sm100_ptx.cuh", "tail_layout.h", "fft_pass.cuh", "fft_pass_split.cuh", "fft_tile.cuh",
            "fft_tile_split.cuh", "fft_queue.cuh", "queue.h", "queue_order.h", "host_schedule.h",
            "tile_pass.h", "layout.h", "mcfft_internal.h"]

@@ -63,7 +63,42 @@ struct alignas(64) QPass {
                         //   k in [t sig_mul / sig_div, ((t + 1) sig_mul - 1) / sig_div],
   int32_t tail_pm;      // radix-R table layout (tail_layout.h)
   int64_t sig_mul, sig_div, sig_kmax;  // k <= sig_kmax; sig_base -1: none
+  // L2 eviction priority of the pass's tile loads and stores (kL2Normal,
+  // kL2EvictFirst, kL2EvictLast).
+  int32_t l2_in, l2_out;
+  const struct QPassAux* aux;  // device; null: none of its features
 };
+
+// Per-pass features kept out of the parameter block (plan-owned device
+// memory, fixed for the plan's life).
+struct QPassAux {
+  // Input read for the last time (an intermediate between passes): once a
+  // tile is in shared memory its source lines are dropped from L2 without
+  // write-back.  Row-input passes only: tile (cb, outer) covers rows
+  // cb * C + r (r < C) of disc_row_bytes at disc_base + outer * disc_so +
+  // row * disc_sc.  disc_base null: none.
+  const char* disc_base;
+  int64_t disc_sc, disc_so;
+  uint32_t disc_row_bytes;
+  int32_t disc_C;
+  // Transforms at unrelated offsets of the user's buffers (descriptors of
+  // one shape that do not follow each other):
+  //  - in_otab / out_otab: the outer (transform) coordinate of tile outer
+  //    index o is otab[o] instead of o (the map's outer stride is the
+  //    offsets' common unit);
+  //  - in_gtab / out_gtab (one-pass 1D groups, whose tiles span several
+  //    transforms): the tile's staging is filled / drained by row gathers /
+  //    scatters of a map whose rows hold one staging row (g_row_bytes),
+  //    column c's rows at gtab[c] + j, j < gin_rows / gout_rows; four
+  //    columns per instruction.
+  const int32_t* in_otab;
+  const int32_t* out_otab;
+  const int32_t* in_gtab;
+  const int32_t* out_gtab;
+  int32_t gin_rows, gout_rows, g_C, g_row_bytes;
+};
+
+constexpr int32_t kL2Normal = 0, kL2EvictFirst = 1, kL2EvictLast = 2;
 
 struct QItem {
   uint32_t pass;
@@ -153,18 +188,38 @@ struct Variant {
 // with tile routine TL; returns the local index of the first item of
 // another pass.  The pass's tables go to shared memory and its layout
 // entries to registers once per run.
-template <class TL, bool SPLIT, class X>
+// Drops the source lines of tile t of a pass whose input is read for the
+// last time (QPassAux::disc_base); the consumer threads share the lines.
+// Runs once the tile's load has completed.
+__device__ __forceinline__ void discard_tile(const QPassAux& X, int64_t col_blocks, int64_t t,
+                                             int ctid, int nct) {
+  const int64_t cb = t % col_blocks, outer = t / col_blocks;
+  const uint32_t per_row = X.disc_row_bytes >> 7;
+  const uint32_t lines = per_row * (uint32_t)X.disc_C;
+  const char* base = X.disc_base + outer * X.disc_so + cb * X.disc_C * X.disc_sc;
+  for (uint32_t i = (uint32_t)ctid; i < lines; i += (uint32_t)nct) {
+    const uint32_t r = i / per_row, l = i - r * per_row;
+    tile::discard_l2_line(base + r * X.disc_sc + ((int64_t)l << 7));
+  }
+}
+
+// RESIDENT: the pass's tables are already in shared memory (x points at
+// them); otherwise they are loaded here, at the start of the run.
+template <class TL, bool SPLIT, bool RESIDENT = false, class X>
 __device__ __forceinline__ int64_t run_items(const QArgs& a, uint32_t pi, const X& x,
                                              uint8_t* smem, uint64_t* full, uint64_t* outrdy,
                                              int ctid, int64_t k, int64_t nlocal,
                                              uint32_t& mphase) {
-  static_assert(!TL::T::TW_SMEM || TL::T::TW_ROWS * 128 <= QueueSmem::TWS_BYTES, "stage rows");
+  static_assert(RESIDENT || !TL::T::TW_SMEM || TL::T::TW_ROWS * 128 <= QueueSmem::TWS_BYTES,
+                "stage rows");
   const QPass& P = a.pass[pi];
   const int64_t G = gridDim.x;
-  // every consumer is past the previous tile's last barrier, so nobody
-  // still reads the old tables
-  TL::tables(P, smem + QueueSmem::OFF_TAIL, smem + QueueSmem::OFF_TWS, ctid);
-  tile::named_bar(1, TL::NCT);
+  if constexpr (!RESIDENT) {
+    // every consumer is past the previous tile's last barrier, so nobody
+    // still reads the old tables
+    TL::tables(P, smem + QueueSmem::OFF_TAIL, smem + QueueSmem::OFF_TWS, ctid);
+    tile::named_bar(1, TL::NCT);
+  }
   uint2 ient[TL::NIT_P];
   uint32_t eent[TL::NST][TL::NIT_E];
   TL::entries(P, ctid, ient, eent);
@@ -174,6 +229,7 @@ __device__ __forceinline__ int64_t run_items(const QArgs& a, uint32_t pi, const 
   for (;;) {
     const int b = (int)(k & 1);
     const int64_t t = a.items[blockIdx.x + k * G].tile;
+    if (P.aux && P.aux->disc_base) discard_tile(*P.aux, P.col_blocks, t, ctid, TL::NCT);
     if constexpr (SPLIT) {
       TL::run(P, x, ctid, b, t % P.col_blocks, k, mphase, ient, eent);
     } else {
@@ -188,6 +244,136 @@ __device__ __forceinline__ int64_t run_items(const QArgs& a, uint32_t pi, const 
     }
     if (*abort_flag) return nlocal;
   }
+}
+
+// A gathered tile: staging row (j, c) of g_row_bytes (rows j, columns c
+// innermost, no swizzle) is buffer row gtab[c] + j; four columns per
+// gather.
+__device__ __forceinline__ void gather_tile(const CUtensorMap* map, const QPassAux& X,
+                                            const int32_t* gtab, uint32_t dst, uint64_t* bar) {
+  for (int c = 0; c < X.g_C; c += 4) {
+    const int32_t r0 = gtab[c], r1 = gtab[c + 1], r2 = gtab[c + 2], r3 = gtab[c + 3];
+    for (int j = 0; j < X.gin_rows; ++j)
+      tile::tma_gather4(map, dst + (uint32_t)((j * X.g_C + c) * X.g_row_bytes), bar, r0 + j,
+                        r1 + j, r2 + j, r3 + j);
+  }
+}
+__device__ __forceinline__ void scatter_tile(const CUtensorMap* map, const QPassAux& X,
+                                             const int32_t* gtab, uint32_t src) {
+  for (int c = 0; c < X.g_C; c += 4) {
+    const int32_t r0 = gtab[c], r1 = gtab[c + 1], r2 = gtab[c + 2], r3 = gtab[c + 3];
+    for (int j = 0; j < X.gout_rows; ++j)
+      tile::tma_scatter4(map, src + (uint32_t)((j * X.g_C + c) * X.g_row_bytes), r0 + j, r1 + j,
+                         r2 + j, r3 + j);
+  }
+  asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+}
+
+// The producer warp's event loop (one thread): store finished tiles as
+// soon as the consumers release them; load the next tile once its buffer is
+// free and its dependency is met.  Never blocks on one while the other
+// could proceed.
+__device__ __forceinline__ void producer_loop(const QArgs& a, uint32_t sS0, uint32_t sS1,
+                                              uint64_t* full, uint64_t* outrdy,
+                                              volatile int* abort_flag, int64_t nlocal) {
+  const int64_t G = gridDim.x;
+  const uint64_t pol_first = tile::policy_evict_first(), pol_last = tile::policy_evict_last();
+  auto pol = [&](int32_t h) -> uint64_t {
+    return h == kL2EvictFirst ? pol_first : h == kL2EvictLast ? pol_last : 0ull;
+  };
+  int64_t il = 0, is = 0;  // next local item to load / to store
+  int64_t sig = -1;        // stored item whose completion is still to be signalled
+  bool idle = false;       // no progress since idle_since (global timer, ns)
+  uint32_t idle_since = 0;
+  // Completion of a producing tile: its bulk store has finished writing,
+  // then a release add on every key it covers.
+  auto signal = [&](int64_t k) {
+    const QItem it = a.items[blockIdx.x + k * G];
+    const QPass& P = a.pass[it.pass];
+    tile::tma_store_wait_all();
+    queue::fence_proxy_async_global();
+    const int64_t k0 = (int64_t)it.tile * P.sig_mul / P.sig_div;
+    int64_t k1 = ((int64_t)it.tile * P.sig_mul + P.sig_mul - 1) / P.sig_div;
+    if (k1 > P.sig_kmax) k1 = P.sig_kmax;
+    for (int64_t key = k0; key <= k1; ++key)
+      queue::red_release_add(a.counters + P.sig_base + key, 1);
+  };
+  while (is < nlocal) {
+    bool moved = false;
+    if (is < il && queue::mbar_test(&outrdy[is & 1], (uint32_t)(is >> 1) & 1u)) {
+      const QItem it = a.items[blockIdx.x + is * G];
+      const QPass& P = a.pass[it.pass];
+      const uint32_t src = (is & 1) ? sS1 : sS0;
+      const int64_t cb = it.tile % P.col_blocks, outer = it.tile / P.col_blocks;
+      const QPassAux* X = P.aux;
+      if (X && X->out_gtab) {
+        scatter_tile(&P.tmap_out, *X, X->out_gtab + cb * X->g_C, src);
+      } else {
+        int32_t crd[5];
+        tile::tile_coords(P.out_cmul, P.out_omul, cb,
+                          X && X->out_otab ? X->out_otab[outer] : outer, crd);
+        tile::tma_store_pol(&P.tmap_out, P.out_ndims, crd, src, pol(P.l2_out));
+      }
+      tile::tma_store_wait_read();
+      if (sig >= 0) signal(sig);
+      sig = P.sig_base >= 0 ? is : -1;
+      ++is;
+      moved = true;
+    }
+    if (il < nlocal && il < is + 2 && !*abort_flag) {
+      const QItem it = a.items[blockIdx.x + il * G];
+      const QPass& P = a.pass[it.pass];
+      const int64_t outer = it.tile / P.col_blocks;
+      bool ready = true;
+      if (P.wait_base >= 0) {
+        ready = queue::ld_acquire(a.counters + P.wait_base + outer) >= P.wait_count;
+        if (ready) queue::fence_proxy_async_global();
+      }
+      if (ready) {
+        const uint32_t dst = (il & 1) ? sS1 : sS0;
+        const int64_t cb = it.tile % P.col_blocks;
+        sm100::mbar_arrive_expect_tx(&full[il & 1], P.in_tile_bytes);
+        const QPassAux* X = P.aux;
+        if (X && X->in_gtab) {
+          gather_tile(&P.tmap_in, *X, X->in_gtab + cb * X->g_C, dst, &full[il & 1]);
+        } else {
+          int32_t crd[5];
+          tile::tile_coords(P.in_cmul, P.in_omul, cb,
+                            X && X->in_otab ? X->in_otab[outer] : outer, crd);
+          tile::tma_load_pol(&P.tmap_in, P.in_ndims, crd, dst, &full[il & 1], pol(P.l2_in));
+        }
+        ++il;
+        moved = true;
+      }
+    }
+    // Signal after the attempt to issue the next load, so that waiting
+    // for the store's completion does not delay it (and never later: the
+    // next load may depend on this very tile).
+    if (sig >= 0) {
+      signal(sig);
+      sig = -1;
+    }
+    if (moved) {
+      idle = false;
+    } else {
+      const uint32_t now = sm100::globaltimer_ns();
+      if (!idle) {
+        idle = true;
+        idle_since = now;
+      }
+      if (*abort_flag || now - idle_since > kWaitLimit) {
+        *abort_flag = 1;
+        break;
+      }
+      __nanosleep(32);
+    }
+  }
+  if (sig >= 0) signal(sig);
+  tile::tma_store_wait_all();
+  // Loads issued but not consumed (abort path) must land before the
+  // CTA's shared memory is released.
+  for (int64_t k = is; k < il; ++k)
+    sm100::mbar_wait_bounded(&full[k & 1], (uint32_t)(k >> 1) & 1u, kWaitLimit);
 }
 
 template <int V>
@@ -274,89 +460,7 @@ __global__ void __maxnreg__(96) fft_queue(const __grid_constant__ QArgs a) {
   const SplitCtx xs{x, base_u + Q::OFF_B + 2048, red};
 
   if (producer) {
-    // ------------------------------------------------------------- producer
-    // Event loop: store finished tiles as soon as the consumers release
-    // them; load the next tile once its buffer is free and its dependency
-    // is met.  Never blocks on one while the other could proceed.
-    if (lane == 0) {
-      int64_t il = 0, is = 0;  // next local item to load / to store
-      int64_t sig = -1;        // stored item whose completion is still to be signalled
-      bool idle = false;       // no progress since idle_since (global timer, ns)
-      uint32_t idle_since = 0;
-      // Completion of a producing tile: its bulk store has finished writing,
-      // then a release add on every key it covers.
-      auto signal = [&](int64_t k) {
-        const QItem it = a.items[blockIdx.x + k * G];
-        const QPass& P = a.pass[it.pass];
-        tile::tma_store_wait_all();
-        queue::fence_proxy_async_global();
-        const int64_t k0 = (int64_t)it.tile * P.sig_mul / P.sig_div;
-        int64_t k1 = ((int64_t)it.tile * P.sig_mul + P.sig_mul - 1) / P.sig_div;
-        if (k1 > P.sig_kmax) k1 = P.sig_kmax;
-        for (int64_t key = k0; key <= k1; ++key)
-          queue::red_release_add(a.counters + P.sig_base + key, 1);
-      };
-      while (is < nlocal) {
-        bool moved = false;
-        if (is < il && queue::mbar_test(&outrdy[is & 1], (uint32_t)(is >> 1) & 1u)) {
-          const QItem it = a.items[blockIdx.x + is * G];
-          const QPass& P = a.pass[it.pass];
-          int32_t crd[5];
-          tile::tile_coords(P.out_cmul, P.out_omul, it.tile % P.col_blocks, it.tile / P.col_blocks, crd);
-          tile::tma_store(&P.tmap_out, P.out_ndims, crd, (is & 1) ? sS1 : sS0);
-          tile::tma_store_wait_read();
-          if (sig >= 0) signal(sig);
-          sig = P.sig_base >= 0 ? is : -1;
-          ++is;
-          moved = true;
-        }
-        if (il < nlocal && il < is + 2 && !*abort_flag) {
-          const QItem it = a.items[blockIdx.x + il * G];
-          const QPass& P = a.pass[it.pass];
-          const int64_t outer = it.tile / P.col_blocks;
-          bool ready = true;
-          if (P.wait_base >= 0) {
-            ready = queue::ld_acquire(a.counters + P.wait_base + outer) >= P.wait_count;
-            if (ready) queue::fence_proxy_async_global();
-          }
-          if (ready) {
-            int32_t crd[5];
-            tile::tile_coords(P.in_cmul, P.in_omul, it.tile % P.col_blocks, outer, crd);
-            sm100::mbar_arrive_expect_tx(&full[il & 1], P.in_tile_bytes);
-            tile::tma_load(&P.tmap_in, P.in_ndims, crd, (il & 1) ? sS1 : sS0, &full[il & 1]);
-            ++il;
-            moved = true;
-          }
-        }
-        // Signal after the attempt to issue the next load, so that waiting
-        // for the store's completion does not delay it (and never later: the
-        // next load may depend on this very tile).
-        if (sig >= 0) {
-          signal(sig);
-          sig = -1;
-        }
-        if (moved) {
-          idle = false;
-        } else {
-          const uint32_t now = sm100::globaltimer_ns();
-          if (!idle) {
-            idle = true;
-            idle_since = now;
-          }
-          if (*abort_flag || now - idle_since > kWaitLimit) {
-            *abort_flag = 1;
-            break;
-          }
-          __nanosleep(32);
-        }
-      }
-      if (sig >= 0) signal(sig);
-      tile::tma_store_wait_all();
-      // Loads issued but not consumed (abort path) must land before the
-      // CTA's shared memory is released.
-      for (int64_t k = is; k < il; ++k)
-        sm100::mbar_wait_bounded(&full[k & 1], (uint32_t)(k >> 1) & 1u, kWaitLimit);
-    }
+    if (lane == 0) queue::producer_loop(a, sS0, sS1, full, outrdy, abort_flag, nlocal);
     __syncwarp();
   } else {
     // ------------------------------------------------------------ consumers
@@ -399,6 +503,139 @@ __global__ void __maxnreg__(96) fft_queue(const __grid_constant__ QArgs a) {
 #undef MCFFT_QCASE
           default: *abort_flag = 1; break;
         }
+      }
+      if (*abort_flag) break;
+    }
+  }
+  __syncthreads();
+  if (tid == 0 && *abort_flag && a.status) atomicExch(a.status, kStatusTimeout);
+  if (producer) sm100::tmem_dealloc(tmem_base, TMEM_COLS);
+}
+
+namespace queue {
+
+// The tile routine of variant V (see variant_of).
+template <int V, bool SPLIT>
+struct VariantTile;
+template <int V>
+struct VariantTile<V, false> {
+  using VV = Variant<V>;
+  using type = F16Tile<VV::L, VV::R, (VV::ALT ? 8192 : 16384) / VV::L, VV::PT, 16>;
+};
+template <int V>
+struct VariantTile<V, true> {
+  using VV = Variant<V>;
+  using type = SplitTile<VV::L, VV::R, 8192 / VV::L, VV::PT, 16, VV::ALT>;
+};
+
+}  // namespace queue
+
+// Shared memory of a fused pair of passes: the batch kernel's three tile
+// buffers and DFT-16 matrices, then both passes' tables side by side.
+template <bool SPLIT, int V1, int V2>
+struct FusedSmem {
+  using TL1 = typename queue::VariantTile<V1, SPLIT>::type;
+  using TL2 = typename queue::VariantTile<V2, SPLIT>::type;
+  static constexpr int OFF_S0 = QueueSmem::OFF_S0;
+  static constexpr int OFF_S1 = QueueSmem::OFF_S1;
+  static constexpr int OFF_A = QueueSmem::OFF_A;
+  static constexpr int OFF_B = QueueSmem::OFF_B;
+  static constexpr int OFF_TAIL1 = OFF_B + 4096;
+  static constexpr int OFF_TWS1 = OFF_TAIL1 + TL1::T::TAIL_BYTES;
+  static constexpr int OFF_TAIL2 = OFF_TWS1 + TL1::T::TWS_BYTES;
+  static constexpr int OFF_TWS2 = OFF_TAIL2 + TL2::T::TAIL_BYTES;
+  static constexpr int OFF_BAR = OFF_TWS2 + TL2::T::TWS_BYTES;
+  static constexpr int SMEM_BYTES = OFF_BAR + 256;
+  static_assert(SMEM_BYTES <= 232448, "shared memory budget");
+};
+
+// A four-step pair of passes (pass 0 on tile variant V1 with the four-step
+// twiddle, pass 1 on V2) in one persistent launch: the batch queue's
+// producer, dependency counters and item order, restricted to the two
+// variants, with both passes' tables resident in shared memory so that a
+// CTA may switch pass every few tiles at no cost.  The host orders the
+// items so that a transform's second pass follows its first pass closely
+// and the intermediate is still in L2 when it is read (the passes' L2
+// policies and scratch discards keep it there and keep it from being
+// written back).  Launched cooperatively, like the batch kernel.
+template <bool SPLIT, int V1, int V2>
+__global__ void __maxnreg__(96) fft_fused(const __grid_constant__ QArgs a) {
+  constexpr int NCW = 16, NCT = NCW * 32, NMTMAX = 8;
+  constexpr int TMEM_COLS = 256;
+  using F = FusedSmem<SPLIT, V1, V2>;
+  using TL1 = typename F::TL1;
+  using TL2 = typename F::TL2;
+  extern __shared__ uint8_t smem[];
+  const uint32_t base_u = sm100::smem_u32(smem);
+  const uint32_t sS0 = base_u + F::OFF_S0, sS1 = base_u + F::OFF_S1, sA = base_u + F::OFF_A;
+  const uint32_t bS0 = sS0 - kWinBase, bS1 = sS1 - kWinBase, bA = sA - kWinBase;
+  if ((base_u & 1023u) != 0 || ((bS0 | bS1 | bA) & (uint32_t)(QueueSmem::STAGE_BYTES - 1)) != 0 ||
+      a.npass != 2) {
+    if (threadIdx.x == 0 && a.status) atomicExch(a.status, kStatusLayout);
+    return;
+  }
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + F::OFF_BAR);  // [2]
+  uint64_t* outrdy = full + 2;                                      // [2]
+  uint64_t* mmab = full + 4;                                        // [up to 16]
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(full + 4 + 16);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(full + 4 + 17);
+  uint32_t* red = reinterpret_cast<uint32_t*>(full + 4 + 18);       // [2] split: tile maxima
+  const int tid = threadIdx.x;
+  const int warp = tid >> 5, lane = tid & 31;
+  const bool producer = warp == NCW;
+  const int64_t G = gridDim.x;
+  const int64_t nlocal = a.nitems > blockIdx.x ? (a.nitems - blockIdx.x + G - 1) / G : 0;
+
+  if (producer) {
+    if (lane == 0) {
+      sm100::mbar_init(&full[0], 1);
+      sm100::mbar_init(&full[1], 1);
+      sm100::mbar_init(&outrdy[0], 1);
+      sm100::mbar_init(&outrdy[1], 1);
+      for (int m = 0; m < NMTMAX; ++m) sm100::mbar_init(&mmab[m], 1);
+      *abort_flag = 0;
+      red[0] = 0u;
+      red[1] = 0u;
+      sm100::fence_mbar_init();
+    }
+    __syncwarp();
+    sm100::tmem_alloc(tmem_slot, TMEM_COLS);
+    sm100::tmem_relinquish();
+  } else {
+    for (int i = tid; i < 128; i += NCT) {
+      *reinterpret_cast<uint4*>(smem + F::OFF_B + 16 * i) = __ldg(a.bmat + i);
+      if (SPLIT) *reinterpret_cast<uint4*>(smem + F::OFF_B + 2048 + 16 * i) = __ldg(a.bmat_lo + i);
+    }
+    TL1::tables(a.pass[0], smem + F::OFF_TAIL1, smem + F::OFF_TWS1, tid);
+    TL2::tables(a.pass[1], smem + F::OFF_TAIL2, smem + F::OFF_TWS2, tid);
+  }
+  sm100::fence_proxy_async_smem();
+  sm100::tc_fence_before();
+  __syncthreads();
+  sm100::tc_fence_after();
+  const uint32_t tmem_base = *tmem_slot;
+  const TileCtx x1{sS0, sS1, sA, base_u + F::OFF_B, base_u + F::OFF_TAIL1, base_u + F::OFF_TWS1,
+                   bS0, bS1, bA, tmem_base, mmab, abort_flag};
+  const TileCtx x2{sS0, sS1, sA, base_u + F::OFF_B, base_u + F::OFF_TAIL2, base_u + F::OFF_TWS2,
+                   bS0, bS1, bA, tmem_base, mmab, abort_flag};
+
+  if (producer) {
+    if (lane == 0) queue::producer_loop(a, sS0, sS1, full, outrdy, abort_flag, nlocal);
+    __syncwarp();
+  } else {
+    uint32_t mphase = 0;  // bit m: phase of mmab[m]
+    for (int64_t k = 0; k < nlocal;) {
+      if (!sm100::mbar_wait_bounded(&full[k & 1], (uint32_t)(k >> 1) & 1u, kWaitLimit)) *abort_flag = 1;
+      if (*abort_flag) break;
+      const uint32_t pi = a.items[blockIdx.x + k * G].pass;
+      if constexpr (SPLIT) {
+        const SplitCtx s1{x1, base_u + F::OFF_B + 2048, red};
+        const SplitCtx s2{x2, base_u + F::OFF_B + 2048, red};
+        k = pi == 0 ? queue::run_items<TL1, true, true>(a, 0, s1, smem, full, outrdy, tid, k, nlocal, mphase)
+                    : queue::run_items<TL2, true, true>(a, 1, s2, smem, full, outrdy, tid, k, nlocal, mphase);
+      } else {
+        k = pi == 0 ? queue::run_items<TL1, false, true>(a, 0, x1, smem, full, outrdy, tid, k, nlocal, mphase)
+                    : queue::run_items<TL2, false, true>(a, 1, x2, smem, full, outrdy, tid, k, nlocal, mphase);
       }
       if (*abort_flag) break;
     }

@@ -141,6 +141,99 @@ __device__ __forceinline__ void tma_store(const CUtensorMap* map, int nd, const 
         : "memory");
   asm volatile("cp.async.bulk.commit_group;" ::: "memory");
 }
+// The same with an L2 cache policy (createpolicy) attached: `pol` 0 means
+// none.  Used by the batch kernels to keep an intermediate resident in L2
+// while the input and output stream through it.
+__device__ __forceinline__ void tma_load_pol(const CUtensorMap* map, int nd, const int32_t* crd,
+                                             uint32_t dst, uint64_t* bar, uint64_t pol) {
+  if (!pol) {
+    tma_load(map, nd, crd, dst, bar);
+    return;
+  }
+  const uint64_t m = reinterpret_cast<uint64_t>(map);
+  const uint32_t mb = sm100::smem_u32(bar);
+  if (nd == 3)
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint"
+        " [%0], [%1, {%2, %3, %4}], [%5], %6;" ::"r"(dst),
+        "l"(m), "r"(crd[0]), "r"(crd[1]), "r"(crd[2]), "r"(mb), "l"(pol)
+        : "memory");
+  else if (nd == 4)
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint"
+        " [%0], [%1, {%2, %3, %4, %5}], [%6], %7;" ::"r"(dst),
+        "l"(m), "r"(crd[0]), "r"(crd[1]), "r"(crd[2]), "r"(crd[3]), "r"(mb), "l"(pol)
+        : "memory");
+  else
+    asm volatile(
+        "cp.async.bulk.tensor.5d.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint"
+        " [%0], [%1, {%2, %3, %4, %5, %6}], [%7], %8;" ::"r"(dst),
+        "l"(m), "r"(crd[0]), "r"(crd[1]), "r"(crd[2]), "r"(crd[3]), "r"(crd[4]), "r"(mb), "l"(pol)
+        : "memory");
+}
+__device__ __forceinline__ void tma_store_pol(const CUtensorMap* map, int nd, const int32_t* crd,
+                                              uint32_t src, uint64_t pol) {
+  if (!pol) {
+    tma_store(map, nd, crd, src);
+    return;
+  }
+  const uint64_t m = reinterpret_cast<uint64_t>(map);
+  if (nd == 3)
+    asm volatile(
+        "cp.async.bulk.tensor.3d.global.shared::cta.bulk_group.L2::cache_hint [%0, {%1, %2, %3}], [%4], %5;" ::"l"(m),
+        "r"(crd[0]), "r"(crd[1]), "r"(crd[2]), "r"(src), "l"(pol)
+        : "memory");
+  else if (nd == 4)
+    asm volatile(
+        "cp.async.bulk.tensor.4d.global.shared::cta.bulk_group.L2::cache_hint [%0, {%1, %2, %3, %4}], [%5], %6;" ::"l"(m),
+        "r"(crd[0]), "r"(crd[1]), "r"(crd[2]), "r"(crd[3]), "r"(src), "l"(pol)
+        : "memory");
+  else
+    asm volatile(
+        "cp.async.bulk.tensor.5d.global.shared::cta.bulk_group.L2::cache_hint [%0, {%1, %2, %3, %4, %5}], [%6], %7;" ::"l"(m),
+        "r"(crd[0]), "r"(crd[1]), "r"(crd[2]), "r"(crd[3]), "r"(crd[4]), "r"(src), "l"(pol)
+        : "memory");
+  asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+}
+// Row gathers and scatters of a 2D tensor map whose rows hold E points
+// (box: E x 1): four rows at the given row coordinates, placed one after
+// another (4 x row bytes) at dst / read from src.  For passes whose
+// columns (transforms) lie at unrelated offsets of the buffer.
+__device__ __forceinline__ void tma_gather4(const CUtensorMap* map, uint32_t dst, uint64_t* bar,
+                                            int32_t r0, int32_t r1, int32_t r2, int32_t r3) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile::gather4.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3, %4, %5, %6}], [%7];" ::"r"(dst),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(0), "r"(r0), "r"(r1), "r"(r2), "r"(r3),
+      "r"(sm100::smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ void tma_scatter4(const CUtensorMap* map, uint32_t src, int32_t r0,
+                                             int32_t r1, int32_t r2, int32_t r3) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.global.shared::cta.tile::scatter4.bulk_group"
+      " [%0, {%1, %2, %3, %4, %5}], [%6];" ::"l"(reinterpret_cast<uint64_t>(map)),
+      "r"(0), "r"(r0), "r"(r1), "r"(r2), "r"(r3), "r"(src)
+      : "memory");
+}
+// L2 policies for all accesses of an instruction: evict first (streamed
+// data) or evict last (data read again soon).
+__device__ __forceinline__ uint64_t policy_evict_first() {
+  uint64_t p;
+  asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+__device__ __forceinline__ uint64_t policy_evict_last() {
+  uint64_t p;
+  asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+// Drops one 128-byte line from L2 without writing it back (its contents
+// become undefined): for an intermediate that has been read for the last
+// time.
+__device__ __forceinline__ void discard_l2_line(const void* p) {
+  asm volatile("discard.global.L2 [%0], 128;" ::"l"(p) : "memory");
+}
 __device__ __forceinline__ void tma_store_wait_read() {
   asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
 }

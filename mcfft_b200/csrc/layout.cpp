@@ -113,8 +113,21 @@ uint32_t Staging::offset(uint32_t pos, uint32_t c) const {
   return raw ^ (((raw >> 7) & swz) << 4);
 }
 
+namespace {
+Staging make_staging_sw(Kind kind, int L, int C, int elem, int64_t sp, int64_t sc, int64_t so,
+                        int64_t ncols, int64_t nouter, int pmid);
+}  // namespace
+
 Staging make_staging(Kind kind, int L, int C, int elem, int64_t sp, int64_t sc, int64_t so,
-                     int64_t ncols, int64_t nouter, int pmid) {
+                     int64_t ncols, int64_t nouter, int pmid, bool noswz) {
+  Staging s = make_staging_sw(kind, L, C, elem, sp, sc, so, ncols, nouter, pmid);
+  if (noswz) s.swz = 0;
+  return s;
+}
+
+namespace {
+Staging make_staging_sw(Kind kind, int L, int C, int elem, int64_t sp, int64_t sc, int64_t so,
+                        int64_t ncols, int64_t nouter, int pmid) {
   Staging s;
   s.kind = kind;
   s.L = L;
@@ -197,6 +210,7 @@ Staging make_staging(Kind kind, int L, int C, int elem, int64_t sp, int64_t sc, 
   }
   return s;
 }
+}  // namespace
 
 namespace {
 
@@ -445,7 +459,8 @@ std::string PassLayout::describe() const {
 
 bool build(PassLayout* pl, int L, int R, int C, Kind in_kind, Kind out_kind, int in_elem,
            int out_elem, int64_t in_sp, int64_t in_sc, int64_t in_so, int64_t out_sp,
-           int64_t out_sc, int64_t out_so, int64_t ncols, int64_t nouter, std::string* err) {
+           int64_t out_sc, int64_t out_so, int64_t ncols, int64_t nouter, std::string* err,
+           int unsw) {
   PassLayout& p = *pl;
   p = PassLayout();
   p.L = L; p.R = R; p.C = C;
@@ -467,8 +482,10 @@ bool build(PassLayout* pl, int L, int R, int C, Kind in_kind, Kind out_kind, int
   }
   if (in_kind == COL && (ncols % std::min(C, 128 / in_elem))) { *err = "ncols"; return false; }
   if (out_kind == COL && (ncols % std::min(C, 128 / out_elem))) { *err = "ncols"; return false; }
-  p.in = make_staging(in_kind, L, C, in_elem, in_sp, in_sc, in_so, ncols, nouter);
-  p.out = make_staging(out_kind, L, C, out_elem, out_sp, out_sc, out_so, ncols, nouter);
+  p.in = make_staging(in_kind, L, C, in_elem, in_sp, in_sc, in_so, ncols, nouter, -1,
+                      (unsw & 1) != 0);
+  p.out = make_staging(out_kind, L, C, out_elem, out_sp, out_sc, out_so, ncols, nouter, -1,
+                       (unsw & 2) != 0);
   Ctx x{pl, ilog2(p.NV), ilog2(C), ilog2(R)};
 
   // Candidate bit ids for the low row bits.
@@ -662,7 +679,8 @@ bool build(PassLayout* pl, int L, int R, int C, Kind in_kind, Kind out_kind, int
   const int epi_weight = 16 * nst;  // epilogue instructions per row-warp vs prologue per item-warp
   for (int pm : pmids) {
     if (total_best <= cands[0].cost * epi_weight / 16.0 + 1e-9) break;  // cannot do better
-    p.in = make_staging(in_kind, L, C, in_elem, in_sp, in_sc, in_so, ncols, nouter, pm);
+    p.in = make_staging(in_kind, L, C, in_elem, in_sp, in_sc, in_so, ncols, nouter, pm,
+                        (unsw & 1) != 0);
     for (size_t ci = 0; ci < std::min<size_t>(cands.size(), permutable ? 32 : 4); ++ci) {
       if (ci > 0 && cands[ci].cost > cands[0].cost + 1e-9) break;
       if (total_best <= cands[0].cost * epi_weight / 16.0 + 1e-9) break;  // found the optimum

@@ -58,8 +58,10 @@ struct Staging {
   int32_t cmul[5]{}, omul[5]{};
 };
 
+// noswz: no TMA swizzle (staging filled by row gathers, whose destinations
+// are not aligned to the swizzle pattern's 1 KB period).
 Staging make_staging(Kind kind, int L, int C, int elem, int64_t sp, int64_t sc, int64_t so,
-                     int64_t ncols, int64_t nouter, int pmid = -1);
+                     int64_t ncols, int64_t nouter, int pmid = -1, bool noswz = false);
 
 // A-operand byte offset of (row r, complex position n) in the SWIZZLE_64B
 // K-major layout (8-row atoms of 512 bytes).
@@ -93,9 +95,12 @@ struct PassLayout {
 
 // Builds the layout of one pass.  out_elem: bytes of an output element.
 // Returns false (with *err) if no layout satisfies the kernel's constraints.
+// unsw: bit 0 / bit 1 -- the input / output staging without swizzle (see
+// make_staging).
 bool build(PassLayout* pl, int L, int R, int C, Kind in_kind, Kind out_kind, int in_elem,
            int out_elem, int64_t in_sp, int64_t in_sc, int64_t in_so, int64_t out_sp,
-           int64_t out_sc, int64_t out_so, int64_t ncols, int64_t nouter, std::string* err);
+           int64_t out_sc, int64_t out_so, int64_t ncols, int64_t nouter, std::string* err,
+           int unsw = 0);
 
 }  // namespace layout
 }  // namespace mcfft

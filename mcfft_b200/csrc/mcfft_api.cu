@@ -56,6 +56,12 @@ struct PassSpec {
   int64_t postN;
   int in_f16, out_f16;
   int64_t in_off, out_off;
+  // Transforms at unrelated offsets of the user's buffers (an indexed
+  // group): the element offset of each outer index (in_so / out_so unused),
+  // or, for a gathered one-pass 1D group (columns = transforms, one outer
+  // index), of each column.  Empty: affine addressing.
+  std::vector<int64_t> in_idx = {}, out_idx = {};
+  bool gather = false;
 };
 
 struct Pass {
@@ -81,6 +87,11 @@ struct Pass {
   int64_t sig_mul = 1, sig_div = 1;
   int wait_count = 0;
   int64_t keys = 0;
+  // Indexed / gathered addressing (PassSpec::in_idx): device tables and the
+  // staging-row geometry the batch kernel reads (QPassAux).
+  const int32_t* in_tab = nullptr;
+  const int32_t* out_tab = nullptr;
+  int gin_rows = 0, gout_rows = 0, g_row_bytes = 0;
 };
 
 // The batch queue of a plan: every pass in one persistent launch.
@@ -93,6 +104,12 @@ struct Queue {
   std::vector<int> wait_base, sig_base;  // per pass
   int grid = 0;
   QArgs* args = nullptr;  // host staging of the parameter block
+  std::vector<const QPassAux*> aux;  // per pass, device (or null)
+  // The kernel: the general batch kernel, or a fused four-step kernel for a
+  // single 1D transform group (fused.cu).
+  const void* fn = nullptr;
+  int smem = 0;
+  bool fused = false;
   // Fault injection for the failure-detection tests (MCFFT_INJECT_STALL at
   // plan time): every dependent pass waits for a producer count that can
   // never be reached, so its tiles time out on the device and the exec
@@ -124,6 +141,11 @@ struct mcfftPlan_st {
   // The plan is meant for the batch queue (several transform groups, or
   // MCFFT_QUEUE=1): its passes take only tile shapes the batch kernel holds.
   bool queue_planned = false;
+  // A group the batch queue cannot run (three-pass 1D lengths).
+  bool no_queue = false;
+  // An indexed transform group (per-transform offsets), which only the
+  // batch queue can run.
+  bool indexed = false;
   // Executable graphs of recent execs, keyed by (in, out, direction): an
   // exec repeated on the same buffers replays its captured launches.
   struct GraphEntry {
@@ -280,6 +302,70 @@ mcfftResult make_stage_rows(mcfftPlan p, int L, int R, double scale, const float
   return MCFFT_SUCCESS;
 }
 
+// Largest power of two dividing every offset (at most 2^20).
+int64_t offsets_unit(const std::vector<int64_t>& v) {
+  int64_t u = int64_t(1) << 20;
+  for (int64_t x : v)
+    while (x % u) u >>= 1;
+  return u;
+}
+
+// Indexed outer dimension of a staging's tensor map (PassSpec::in_idx):
+// stride = the offsets' common unit, extent = the largest offset / unit + 1;
+// `tab` receives offset / unit per outer index.  False if impossible.
+bool index_outer(layout::Staging* st, const std::vector<int64_t>& offs, std::vector<int32_t>* tab) {
+  const int64_t unit = offsets_unit(offs);
+  if ((unit * st->elem) % 16) return false;
+  int d = -1;
+  for (int i = 0; i < st->ndims; ++i)
+    if (st->omul[i] == 1) d = i;
+  if (d < 1) return false;
+  int64_t mx = 0;
+  tab->clear();
+  for (int64_t o : offs) {
+    if (o < 0 || o / unit >= (int64_t(1) << 31)) return false;
+    tab->push_back((int32_t)(o / unit));
+    mx = std::max(mx, o / unit);
+  }
+  st->gdim[d] = (uint64_t)mx + 1;
+  st->gstride_bytes[d] = (uint64_t)(unit * st->elem);
+  return true;
+}
+
+// Row map of a gathered side: rows of the tile staging's E points over the
+// whole buffer (extent: the last transform's end), box E x 1, no swizzle;
+// `tab` receives each column's first row (columns padded to a multiple of
+// C with the last one).  False if an offset is not a whole row.
+bool gather_rows(const layout::Staging& tile_st, int64_t L, int64_t C,
+                 const std::vector<int64_t>& offs, layout::Staging* out, std::vector<int32_t>* tab) {
+  const int64_t E = tile_st.E;
+  if (tile_st.kind != layout::ROW || E * tile_st.elem != 128 || L % E) return false;
+  int64_t end = 0;
+  tab->clear();
+  for (int64_t o : offs) {
+    if (o < 0 || o % E || (o + L) / E >= (int64_t(1) << 31)) return false;
+    tab->push_back((int32_t)(o / E));
+    end = std::max(end, o + L);
+  }
+  while ((int64_t)tab->size() % C) tab->push_back(tab->back());
+  layout::Staging g;
+  g.kind = layout::ROW;
+  g.L = (int)L;
+  g.C = (int)C;
+  g.elem = tile_st.elem;
+  g.E = (int)E;
+  g.row_bytes = 128;
+  g.swz = 0;
+  g.ndims = 2;
+  g.gdim[0] = (uint64_t)E;
+  g.box[0] = (uint32_t)E;
+  g.gdim[1] = (uint64_t)(end / E);
+  g.box[1] = 1;
+  g.gstride_bytes[1] = 128;
+  *out = g;
+  return true;
+}
+
 // Builds a pass on the TMA-fed kernel.  Returns MCFFT_UNSUPPORTED_SIZE when
 // the shape is outside what that kernel handles (the caller falls back).
 mcfftResult add_tile_pass(mcfftPlan p, const PassSpec& s, int only_tile_points = 0) {
@@ -304,18 +390,37 @@ mcfftResult add_tile_pass(mcfftPlan p, const PassSpec& s, int only_tile_points =
   ps.tiled = true;
   TilePass& tp = ps.tp;
   const TileKernel* k = nullptr;
+  std::vector<int32_t> in_tab, out_tab;
+  const bool indexed = s.gather || !s.in_idx.empty() || !s.out_idx.empty();
   for (int oi = 0; oi < 2 && !k; ++oi) {
     const TileKernel* cand =
         find_tile_kernel((int)s.L, s.posttw, p->split, order[oi], s.in_f16 != 0);
     if (!cand) continue;
     if (!p->split && (in_elem != 4 || out_elem != 4)) continue;
     // a plan meant for the batch queue takes only tile shapes the batch
-    // kernel holds (not L = 4096 in 8K-point tiles)
-    if (p->queue_planned && queue_variant(*cand) < 0) continue;
+    // kernel holds (not L = 4096 in 8K-point tiles); indexed passes run
+    // only there, gathered ones with four columns per gather
+    if ((p->queue_planned || indexed) && queue_variant(*cand) < 0) continue;
+    if (s.gather && (cand->C < 4 || ik != layout::ROW || ok != layout::ROW)) continue;
     std::string err;
     if (!tile_layout(&tp.lay, cand->L, cand->R, cand->C, ik, ok, in_elem, out_elem, s.in_sp,
-                     s.in_sc, s.in_so, s.out_sp, s.out_sc, s.out_so, s.ncols, s.nouter, &err))
+                     s.in_sc, s.in_so, s.out_sp, s.out_sc, s.out_so, s.ncols, s.nouter, &err,
+                     s.gather ? 3 : 0))
       continue;
+    if (s.gather) {
+      layout::Staging gi, go;
+      if (!gather_rows(tp.lay.in, s.L, cand->C, s.in_idx, &gi, &in_tab) ||
+          !gather_rows(tp.lay.out, s.L, cand->C, s.out_idx, &go, &out_tab))
+        continue;
+      ps.gin_rows = (int)(s.L / tp.lay.in.E);
+      ps.gout_rows = (int)(s.L / tp.lay.out.E);
+      ps.g_row_bytes = 128;
+      tp.lay.in = gi;
+      tp.lay.out = go;
+    } else {
+      if (!s.in_idx.empty() && !index_outer(&tp.lay.in, s.in_idx, &in_tab)) continue;
+      if (!s.out_idx.empty() && !index_outer(&tp.lay.out, s.out_idx, &out_tab)) continue;
+    }
     if (!tile_check_encode(tp.lay.in, p->status) || !tile_check_encode(tp.lay.out, p->status))
       continue;
     k = cand;
@@ -324,6 +429,17 @@ mcfftResult add_tile_pass(mcfftPlan p, const PassSpec& s, int only_tile_points =
   tp.k = k;
   fill_tile_args(&tp);
   TileArgs& a = tp.args;
+  if (s.gather) a.in_tile_bytes = (uint32_t)(k->L * k->C * in_elem);
+  for (int side = 0; side < 2; ++side) {
+    const std::vector<int32_t>& t = side ? out_tab : in_tab;
+    if (t.empty()) continue;
+    int32_t* d = nullptr;
+    mcfftResult r = plan_alloc(p, &d, t.size() * sizeof(int32_t));
+    if (r) return r;
+    if (cudaMemcpy(d, t.data(), t.size() * sizeof(int32_t), cudaMemcpyHostToDevice) != cudaSuccess)
+      return MCFFT_CUDA_ERROR;
+    (side ? ps.out_tab : ps.in_tab) = d;
+  }
   a.col_blocks = (s.ncols + k->C - 1) / k->C;
   a.ntiles = a.col_blocks * s.nouter;
   a.out_scale = 1.0f;  // unused: the plain form's last 1/16 is in the DFT-16 matrix,
@@ -483,7 +599,9 @@ mcfftResult autotune_group(mcfftPlan p, size_t first, int64_t points) {
   const std::string gk = gpu_key(p);
   std::vector<size_t> todo;
   for (size_t i = first; i < p->passes.size(); ++i) {
-    if (!p->passes[i].tiled) continue;
+    // indexed passes keep the default shape (they run only in the batch
+    // queue, which the tuner's single-pass timing does not model)
+    if (!p->passes[i].tiled || p->passes[i].in_tab || p->passes[i].out_tab) continue;
     const int rec = wisdom_find(gk + "\t" + pass_key(p->passes[i].spec));
     if (!rec) {
       todo.push_back(i);
@@ -535,6 +653,8 @@ mcfftResult add_pass(mcfftPlan p, const PassSpec& s) {
   {
     mcfftResult tr = add_tile_pass(p, s);
     if (tr != MCFFT_UNSUPPORTED_SIZE) return tr;
+    // the direct-load kernels address only affine layouts
+    if (s.gather || !s.in_idx.empty() || !s.out_idx.empty()) return tr;
   }
   const PassKernel* k =
       pick_pass_kernel((int)s.L, s.colfast, s.posttw, p->split, s.ncols, tile_points_env());
@@ -612,6 +732,51 @@ mcfftResult add_pass(mcfftPlan p, const PassSpec& s) {
 constexpr int64_t kMaxSinglePass = 8192;
 constexpr int64_t kMaxTilePass = 4096;  // 1D lengths above run as four-step (split: 2048)
 
+constexpr int64_t kMaxLength1d = int64_t(1) << 27;
+
+// 1D lengths of 2^27 (the reference plans 2^27 in three passes,
+// source/mcfft_1d_device.cpp:762-771): n = n1 * n2 * n3, m = n2 * n3, the
+// four-step split applied twice --
+//   pass 1  n1-point columns j < m (stride m), times W_n^(k1 j), into the
+//           scratch as A[k1][j]
+//   pass 2  in place in the scratch, per row k1: n2-point columns j3 < n3
+//           (stride n3), times W_m^(k2 j3): B[k1][k2][j3]
+//   pass 3  per transform, per k2: n3-point rows of B, columns k1 (stride m
+//           in the scratch), written to X[k1 + n1 k2 + n1 n2 k3] (stride
+//           n1 n2, columns contiguous)
+// Pass 3's outer index (k2) would need a second stride across transforms,
+// so it is one pass per transform.  Such a group never runs in the batch
+// queue.
+mcfftResult build_three_pass(mcfftPlan p, int64_t n, int64_t batch, int64_t in_off,
+                             int64_t out_off) {
+  if (n > kMaxLength1d) return MCFFT_UNSUPPORTED_SIZE;
+  const bool split = p->split;
+  const int in_f16 = split ? ((p->flags & MCFFT_FLAG_INPUT_F16) ? 1 : 0) : 1;
+  const int mid_f16 = split ? 0 : 1;
+  const int lg = ilog2(n), lg1 = lg / 3, lg2 = (lg - lg1) / 2;
+  const int64_t n1 = int64_t(1) << lg1, n2 = int64_t(1) << lg2, n3 = n >> (lg1 + lg2);
+  const int64_t m = n2 * n3;
+  const size_t ebytes = split ? 8 : 4;
+  const int64_t soff = (int64_t)(p->scratch_bytes / ebytes);
+  PassSpec s1{n1, true, true, m, 1, n, m, 1, n, m, batch, kUserIn, kScratch, n,
+              in_f16, mid_f16, in_off, soff};
+  mcfftResult r = add_pass(p, s1);
+  if (r) return r;
+  PassSpec s2{n2, true, true, n3, 1, m, n3, 1, m, n3, batch * n1, kScratch, kScratch, m,
+              mid_f16, mid_f16, soff, soff};
+  r = add_pass(p, s2);
+  if (r) return r;
+  for (int64_t b = 0; b < batch && !r; ++b) {
+    PassSpec s3{n3, false, false, 1, m, n3, n1 * n2, 1, n1, n1, n2, kScratch, kUserOut, 0,
+                mid_f16, split ? 0 : 1, soff + b * n, out_off + b * n};
+    r = add_pass(p, s3);
+  }
+  if (r) return r;
+  p->scratch_bytes += (size_t)n * batch * ebytes;
+  p->no_queue = true;
+  return MCFFT_SUCCESS;
+}
+
 // Appends the passes of one transform group.  `in_buf/out_buf` and offsets
 // locate it inside the user's buffers; the first pass reads in_buf, the
 // last writes out_buf.
@@ -634,7 +799,11 @@ mcfftResult build_group_passes(mcfftPlan p, int ndim, const int64_t* dims, int64
                  in_f16, split ? 0 : 1, in_off, out_off};
       return add_pass(p, s);
     }
-    if (n > kMaxSinglePass * kMaxSinglePass) return MCFFT_UNSUPPORTED_SIZE;
+    // MCFFT_THREE_PASS=1 takes the three-pass plan for every length past one
+    // pass (a test switch: the same code path at sizes that test quickly)
+    const char* three = std::getenv("MCFFT_THREE_PASS");
+    if (n > kMaxSinglePass * kMaxSinglePass || (three && std::atoi(three) != 0 && n >= 4096 * 16))
+      return build_three_pass(p, n, batch, in_off, out_off);
     const int lg = ilog2(n);
     int lg1 = lg / 2;
     if (const char* e = std::getenv("MCFFT_FOURSTEP_N1")) lg1 = ilog2(std::atoll(e));
@@ -743,6 +912,7 @@ void link_group(mcfftPlan p, size_t first, int ndim, const int64_t* dims, int64_
     p->passes[i].level = (int)(i - first);
   }
   if (p->passes.size() - first < 2) return;
+  if (ndim == 1 && p->passes.size() - first != 2) return;  // three-pass: never queued
   for (size_t i = first; i < p->passes.size(); ++i)
     if (!p->passes[i].tiled) return;  // the queue only runs tile passes
   auto C = [&](size_t i) -> int64_t { return p->passes[i].tp.k->C; };
@@ -785,6 +955,110 @@ mcfftResult build_group(mcfftPlan p, int ndim, const int64_t* dims, int64_t batc
   return r;
 }
 
+// An indexed transform group: B transforms of one shape at the element
+// offsets ioff[b] of the input and ooff[b] of the output, in no particular
+// order (descriptors of one shape that do not follow each other).  The same
+// passes as build_group_passes, with per-transform coordinate tables: a
+// one-pass 1D group gathers its tiles' columns (transforms) row by row, the
+// other passes look their outer (transform) coordinate up.  Such a group
+// runs only in the batch kernel.
+mcfftResult build_indexed_group(mcfftPlan p, int ndim, const int64_t* dims,
+                                const std::vector<int64_t>& ioff, const std::vector<int64_t>& ooff,
+                                int* scale_log2) {
+  const size_t first = p->passes.size();
+  const bool split = p->split;
+  const int in_f16 = split ? ((p->flags & MCFFT_FLAG_INPUT_F16) ? 1 : 0) : 1;
+  const int mid_f16 = split ? 0 : 1, out_f16 = split ? 0 : 1;
+  const int64_t B = (int64_t)ioff.size();
+  int64_t total = 1;
+  for (int d = 0; d < ndim; ++d) {
+    if (!is_pow2(dims[d]) || dims[d] < 16) return MCFFT_UNSUPPORTED_SIZE;
+    total *= dims[d];
+  }
+  *scale_log2 = split ? 0 : -ilog2(total);
+  mcfftResult r = MCFFT_SUCCESS;
+  if (ndim == 1) {
+    const int64_t n = dims[0];
+    if (n <= (split ? kMaxTilePass / 2 : kMaxTilePass)) {
+      PassSpec sp{n, false, false, 1, n, 0, 1, n, 0, B, 1, kUserIn, kUserOut, 0,
+                  in_f16, out_f16, 0, 0};
+      sp.in_idx = ioff;
+      sp.out_idx = ooff;
+      sp.gather = true;
+      r = add_pass(p, sp);
+    } else if (n <= kMaxSinglePass * kMaxSinglePass) {
+      const int lg = ilog2(n), lg1 = lg / 2;
+      const int64_t n1 = int64_t(1) << lg1, n2 = n >> lg1;
+      if (n1 < 16 || n2 < 16 || n1 > kMaxSinglePass || n2 > kMaxSinglePass)
+        return MCFFT_UNSUPPORTED_SIZE;
+      const size_t ebytes = split ? 8 : 4;
+      const int64_t soff = (int64_t)(p->scratch_bytes / ebytes);
+      PassSpec s1{n1, true, true, n2, 1, n, n2, 1, n, n2, B, kUserIn, kScratch, n,
+                  in_f16, mid_f16, 0, soff};
+      s1.in_idx = ioff;
+      r = add_pass(p, s1);
+      if (r) return r;
+      PassSpec s2{n2, false, false, 1, n2, n, n1, 1, n, n1, B, kScratch, kUserOut, 0,
+                  mid_f16, out_f16, soff, 0};
+      s2.out_idx = ooff;
+      r = add_pass(p, s2);
+      if (r) return r;
+      p->scratch_bytes += (size_t)n * B * ebytes;
+    } else {
+      return MCFFT_UNSUPPORTED_SIZE;
+    }
+  } else {
+    for (int d = 0; d < ndim; ++d)
+      if (dims[d] > kMaxSinglePass) return MCFFT_UNSUPPORTED_SIZE;
+    if (ndim == 2) {
+      const int64_t nx = dims[0], ny = dims[1];
+      PassSpec s1{ny, false, false, 1, ny, 0, 1, ny, 0, nx, B, kUserIn, kUserOut, 0,
+                  in_f16, mid_f16, 0, 0};
+      s1.in_idx = ioff;
+      s1.out_idx = ooff;
+      r = add_pass(p, s1);
+      if (r) return r;
+      PassSpec s2{nx, true, false, ny, 1, 0, ny, 1, 0, ny, B, kUserOut, kUserOut, 0,
+                  mid_f16, mid_f16, 0, 0};
+      s2.in_idx = ooff;
+      s2.out_idx = ooff;
+      r = add_pass(p, s2);
+    } else if (ndim == 3) {
+      const int64_t nx = dims[0], ny = dims[1], nz = dims[2];
+      PassSpec s1{nz, false, false, 1, nz, 0, 1, nz, 0, nx * ny, B, kUserIn, kUserOut, 0,
+                  in_f16, mid_f16, 0, 0};
+      s1.in_idx = ioff;
+      s1.out_idx = ooff;
+      r = add_pass(p, s1);
+      if (r) return r;
+      std::vector<int64_t> slabs;  // outer (b, x): the x-th slab of transform b
+      for (int64_t b = 0; b < B; ++b)
+        for (int64_t x = 0; x < nx; ++x) slabs.push_back(ooff[b] + x * ny * nz);
+      PassSpec s2{ny, true, false, nz, 1, 0, nz, 1, 0, nz, nx * B, kUserOut, kUserOut, 0,
+                  mid_f16, mid_f16, 0, 0};
+      s2.in_idx = slabs;
+      s2.out_idx = slabs;
+      r = add_pass(p, s2);
+      if (r) return r;
+      PassSpec s3{nx, true, false, ny * nz, 1, 0, ny * nz, 1, 0, ny * nz, B, kUserOut, kUserOut,
+                  0, mid_f16, mid_f16, 0, 0};
+      s3.in_idx = ooff;
+      s3.out_idx = ooff;
+      r = add_pass(p, s3);
+    } else {
+      return MCFFT_INVALID_VALUE;
+    }
+    // the first pass's tiles must not straddle transforms (its dependency
+    // keys count whole tiles per transform)
+    if (!r && p->passes[first].spec.ncols % p->passes[first].tp.k->C != 0)
+      return MCFFT_UNSUPPORTED_SIZE;
+  }
+  if (r) return r;
+  link_group(p, first, ndim, dims, B);
+  p->indexed = true;
+  return MCFFT_SUCCESS;
+}
+
 // Builds the batch queue (every pass of the plan in one persistent launch)
 // for plans of several transform groups (uneven batches) -- or any plan
 // with MCFFT_QUEUE=1; MCFFT_QUEUE=0 disables it -- when every pass runs on
@@ -799,10 +1073,101 @@ mcfftResult build_group(mcfftPlan p, int ndim, const int64_t* dims, int64_t batc
 // a row (its tables stay in shared memory), and the tail of one group's
 // later pass runs beside the next group's first pass instead of waiting on
 // the tiles queued just before it.
+// L2 use of pass i in the batch kernels (MCFFT_L2_HINTS=1; off by default:
+// measured slower on the four-step pair, whose column tiles read half
+// lines that the neighbouring tile reads again): an intermediate another
+// pass reads (the plan's scratch, or the output read again in place) is
+// stored with evict-last priority; data read or written once streams with
+// evict-first.
+bool l2_hints_on() {
+  static const bool on = [] {
+    const char* e = std::getenv("MCFFT_L2_HINTS");
+    return e && std::atoi(e) != 0;
+  }();
+  return on;
+}
+// Scratch lines dropped from L2 after their last read (MCFFT_L2_DISCARD=0:
+// kept, and written back when evicted).
+bool l2_discard_on() {
+  static const bool on = [] {
+    const char* e = std::getenv("MCFFT_L2_DISCARD");
+    return !e || std::atoi(e) != 0;
+  }();
+  return on;
+}
+
+void set_l2_use(mcfftPlan p, size_t i, QPass* Q) {
+  if (!l2_hints_on()) return;
+  const Pass& ps = p->passes[i];
+  const bool read_later = i + 1 < p->passes.size() && p->passes[i + 1].grp == ps.grp &&
+                          p->passes[i + 1].level > 0;
+  Q->l2_out = read_later ? kL2EvictLast : kL2EvictFirst;
+  if (ps.in_buf == kUserIn || ps.in_buf == kScratch) Q->l2_in = kL2EvictFirst;
+}
+
+// Plan-time per-pass features of the batch kernels (QPassAux): a row-input
+// pass reading the scratch drops each tile's source lines from L2 once the
+// tile is loaded (no write-back of a dead intermediate), when its tiles
+// cover whole rows.  Returns the host copy; `any` tells whether it holds
+// anything.
+QPassAux make_aux(mcfftPlan p, size_t i, bool* any) {
+  QPassAux x;
+  std::memset(&x, 0, sizeof(x));
+  *any = false;
+  const Pass& ps = p->passes[i];
+  if (l2_discard_on() && ps.in_buf == kScratch) {
+    const PassSpec& sp = ps.spec;
+    const int64_t C = ps.tp.k->C, eb = ps.in_f16 ? 4 : 8;
+    const int64_t row = sp.L * eb;
+    const char* in_base = static_cast<const char*>(p->scratch) + ps.in_off * eb;
+    if (sp.in_sp == 1 && sp.ncols % C == 0 && row % 128 == 0 && (sp.in_sc * eb) % 128 == 0 &&
+        (sp.in_so * eb) % 128 == 0 && (reinterpret_cast<uintptr_t>(in_base) & 127) == 0) {
+      x.disc_base = in_base;
+      x.disc_sc = sp.in_sc * eb;
+      x.disc_so = sp.in_so * eb;
+      x.disc_row_bytes = (uint32_t)row;
+      x.disc_C = (int32_t)C;
+      *any = true;
+    }
+  }
+  if (ps.in_tab || ps.out_tab) {
+    const bool g = ps.spec.gather;
+    x.in_otab = g ? nullptr : ps.in_tab;
+    x.out_otab = g ? nullptr : ps.out_tab;
+    x.in_gtab = g ? ps.in_tab : nullptr;
+    x.out_gtab = g ? ps.out_tab : nullptr;
+    x.gin_rows = ps.gin_rows;
+    x.gout_rows = ps.gout_rows;
+    x.g_C = ps.tp.k->C;
+    x.g_row_bytes = ps.g_row_bytes;
+    *any = true;
+  }
+  return x;
+}
+
+// A single 1D four-step transform group whose pair of tile variants has a
+// fused kernel runs both passes in one launch of it (MCFFT_FUSED=0: pass by
+// pass), its items ordered in chunks of two tiles per CTA (a transform's
+// second pass follows its first within a few tiles per CTA, while its
+// intermediate is still in L2).
+const FusedKernel* fused_for(mcfftPlan p) {
+  if (const char* e = std::getenv("MCFFT_FUSED"))
+    if (std::atoi(e) == 0) return nullptr;
+  if (p->ngroups != 1 || p->passes.size() != 2 || p->no_queue) return nullptr;
+  const Pass &a = p->passes[0], &b = p->passes[1];
+  if (!a.tiled || !b.tiled || !a.spec.posttw || b.spec.posttw || a.out_buf != kScratch ||
+      b.in_buf != kScratch)
+    return nullptr;
+  const int v1 = queue_variant(*a.tp.k), v2 = queue_variant(*b.tp.k);
+  if (v1 < 0 || v2 < 0) return nullptr;
+  return find_fused(p->split, v1, v2);
+}
+
 mcfftResult build_queue(mcfftPlan p) {
-  bool want = p->ngroups > 1;
-  if (const char* e = std::getenv("MCFFT_QUEUE")) want = std::atoi(e) != 0;
-  if (!want) return MCFFT_SUCCESS;
+  const FusedKernel* fk = fused_for(p);
+  bool want = p->ngroups > 1 || fk || p->indexed;
+  if (const char* e = std::getenv("MCFFT_QUEUE")) want = std::atoi(e) != 0 || fk || p->indexed;
+  if (!want || p->no_queue) return MCFFT_SUCCESS;
   const size_t np = p->passes.size();
   if (np > (size_t)kQueueMaxPasses) return MCFFT_SUCCESS;
   for (const auto& ps : p->passes)
@@ -812,8 +1177,17 @@ mcfftResult build_queue(mcfftPlan p) {
                 (long long)(ps.tiled ? ps.tp.k->L : ps.k->L));
       return MCFFT_SUCCESS;
     }
-  const int maxg = queue_max_grid(p->sms, p->split);
-  if (maxg <= 0) return MCFFT_SUCCESS;
+  Queue& q0 = p->q;
+  q0.fused = fk != nullptr;
+  q0.fn = fk ? fk->fn : nullptr;
+  q0.smem = fk ? fk->smem_bytes : 0;
+  const int maxg = fk ? queue_max_grid_fn(fk->fn, fk->smem_bytes, p->sms)
+                      : queue_max_grid(p->sms, p->split);
+  if (maxg <= 0) {
+    q0.fused = false;
+    q0.fn = nullptr;
+    return MCFFT_SUCCESS;
+  }
   Queue& q = p->q;
   q.wait_base.assign(np, -1);
   q.sig_base.assign(np, -1);
@@ -827,7 +1201,7 @@ mcfftResult build_queue(mcfftPlan p) {
   const int64_t G = maxg;
   // first-pass tiles per CTA queued at a time (a CTA reloads a pass's tables when its
   // consecutive items switch pass)
-  int64_t QC = 16;
+  int64_t QC = fk ? 2 : 16;
   if (const char* e = std::getenv("MCFFT_QUEUE_CHUNK")) QC = std::max<int64_t>(1, std::atoll(e));
   std::vector<QOrderPass> qo(np);
   for (size_t i = 0; i < np; ++i) {
@@ -849,6 +1223,18 @@ mcfftResult build_queue(mcfftPlan p) {
   cudaError_t e = cudaMemcpy(q.items, items.data(), items.size() * sizeof(QItem),
                              cudaMemcpyHostToDevice);
   if (e != cudaSuccess) return cuda_fail(e);
+  q.aux.assign(np, nullptr);
+  for (size_t i = 0; i < np; ++i) {
+    bool any = false;
+    const QPassAux x = make_aux(p, i, &any);
+    if (!any) continue;
+    QPassAux* d = nullptr;
+    r = plan_alloc(p, &d, sizeof(QPassAux));
+    if (r) return r;
+    e = cudaMemcpy(d, &x, sizeof(x), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return cuda_fail(e);
+    q.aux[i] = d;
+  }
   q.nitems = (int64_t)items.size();
   q.ncounters = nc;
   q.grid = (int)std::min<int64_t>(G, q.nitems);
@@ -885,10 +1271,13 @@ mcfftResult exec_queue(mcfftPlan p, const void* in, void* out, int dir, cudaStre
     Q.sig_mul = ps.sig_mul;
     Q.sig_div = ps.sig_div;
     Q.sig_kmax = q.sig_base[i] >= 0 ? p->passes[i + 1].keys - 1 : 0;
+    set_l2_use(p, i, &Q);
+    Q.aux = q.aux[i];
   }
   cudaError_t e = q.ncounters ? cudaMemsetAsync(q.counters, 0, q.ncounters * sizeof(int), st)
                               : cudaSuccess;
-  if (e == cudaSuccess) e = launch_queue(A, q.grid, p->split, st);
+  if (e == cudaSuccess)
+    e = q.fused ? launch_queue_fn(q.fn, q.smem, A, q.grid, st) : launch_queue(A, q.grid, p->split, st);
   if (e == cudaSuccess && std::getenv("MCFFT_DEBUG_SYNC")) {
     e = cudaStreamSynchronize(st);
     fprintf(stderr, "[mcfft] queue: %d passes, %lld items, grid %d: %s\n", A.npass,
@@ -906,6 +1295,7 @@ mcfftResult plan_finish(mcfftPlan p, mcfftPlan* out) {
   mcfftResult r = MCFFT_SUCCESS;
   if (p->scratch_bytes) r = plan_alloc(p, &p->scratch, p->scratch_bytes);
   if (!r) r = build_queue(p);
+  if (!r && p->indexed && !p->q.on) r = MCFFT_UNSUPPORTED_SIZE;
   if (!r) r = cuda_fail(cudaDeviceSynchronize());
   if (r) {
     mcfftPlanDestroy(p);
@@ -1139,19 +1529,21 @@ using namespace mcfft;
 
 extern "C" {
 
-mcfftResult mcfftPlanCreateBatch(mcfftPlan* plan, const mcfftDesc* descs, int count,
-                                 mcfftPrecision precision, unsigned flags) {
-  if (!plan || !descs || count <= 0) return MCFFT_INVALID_VALUE;
-  for (int i = 0; i < count; ++i)
-    if (descs[i].ndim < 1 || descs[i].ndim > 3 || descs[i].batch < 1 || descs[i].in_offset < 0 ||
-        descs[i].out_offset < 0)
-      return MCFFT_INVALID_VALUE;
+}  // extern "C"
+
+namespace mcfft {
+namespace {
+
+// The plan of a batch of descriptors.  by_shape: one group per shape
+// (indexed where its transforms are not contiguous and in order; *indexed
+// tells whether any was); else one group per run of consecutive
+// descriptors of one shape whose data follow each other in both buffers.
+mcfftResult create_batch(mcfftPlan* plan, const mcfftDesc* descs, int count,
+                         mcfftPrecision precision, unsigned flags, bool by_shape, bool* indexed) {
   mcfftPlan p = nullptr;
   mcfftResult r = plan_begin(plan, precision, flags, &p);
   if (r) return r;
   int64_t elements = 0;
-  // Consecutive descriptors of one shape whose data follow each other in
-  // both buffers form one batched group (one set of passes).
   auto points = [](const mcfftDesc& d) {
     int64_t t = 1;
     for (int k = 0; k < d.ndim; ++k) t *= d.dims[k];
@@ -1165,21 +1557,62 @@ mcfftResult mcfftPlanCreateBatch(mcfftPlan* plan, const mcfftDesc* descs, int co
     const int64_t len = g.batch * points(g);
     return same && d.in_offset == g.in_offset + len && d.out_offset == g.out_offset + len;
   };
-  int ngroups = 0;
-  for (int i = 0; i < count; ++ngroups) {
-    mcfftDesc g = descs[i];
-    for (++i; i < count && continues(i, g); ++i) g.batch += descs[i].batch;
+  // Groups: (shape, per-transform input and output offsets) in order of
+  // first appearance.
+  struct Group {
+    mcfftDesc shape;
+    std::vector<int64_t> in, out;
+  };
+  std::vector<Group> groups;
+  if (by_shape) {
+    for (int i = 0; i < count; ++i) {
+      const mcfftDesc& d = descs[i];
+      Group* g = nullptr;
+      for (auto& x : groups) {
+        bool same = x.shape.ndim == d.ndim;
+        for (int k = 0; k < d.ndim && same; ++k) same = x.shape.dims[k] == d.dims[k];
+        if (same) g = &x;
+      }
+      if (!g) {
+        groups.push_back(Group{d, {}, {}});
+        g = &groups.back();
+      }
+      const int64_t n = points(d);
+      for (int64_t b = 0; b < d.batch; ++b) {
+        g->in.push_back(d.in_offset + b * n);
+        g->out.push_back(d.out_offset + b * n);
+      }
+    }
+  } else {
+    for (int i = 0; i < count;) {
+      mcfftDesc g = descs[i];
+      for (++i; i < count && continues(i, g); ++i) g.batch += descs[i].batch;
+      const int64_t n = points(g);
+      Group x{g, {}, {}};
+      for (int64_t b = 0; b < g.batch; ++b) {
+        x.in.push_back(g.in_offset + b * n);
+        x.out.push_back(g.out_offset + b * n);
+      }
+      groups.push_back(x);
+    }
   }
-  p->queue_planned = ngroups > 1;
+  p->queue_planned = groups.size() > 1;
   if (const char* e = std::getenv("MCFFT_QUEUE")) p->queue_planned = std::atoi(e) != 0;
-  for (int i = 0; i < count && !r;) {
-    mcfftDesc g = descs[i];
-    int j = i + 1;
-    for (; j < count && continues(j, g); ++j) g.batch += descs[j].batch;
+  for (size_t gi = 0; gi < groups.size() && !r; ++gi) {
+    const Group& g = groups[gi];
+    const int64_t n = points(g.shape), B = (int64_t)g.in.size();
+    bool affine = true;
+    for (int64_t b = 0; b < B && affine; ++b)
+      affine = g.in[b] == g.in[0] + b * n && g.out[b] == g.out[0] + b * n;
     int sl = 0;
-    r = build_group(p, g.ndim, g.dims, g.batch, g.in_offset, g.out_offset, &sl);
-    elements += g.batch * points(g);
-    if (i == 0) {
+    if (affine) {
+      r = build_group(p, g.shape.ndim, g.shape.dims, B, g.in[0], g.out[0], &sl);
+    } else {
+      *indexed = true;
+      r = build_indexed_group(p, g.shape.ndim, g.shape.dims, g.in, g.out, &sl);
+    }
+    elements += B * n;
+    if (gi == 0) {
       p->info.ndim = descs[0].ndim;
       for (int d = 0; d < 3; ++d) p->info.dims[d] = d < descs[0].ndim ? descs[0].dims[d] : 1;
       p->info.batch = descs[0].batch;
@@ -1187,7 +1620,6 @@ mcfftResult mcfftPlanCreateBatch(mcfftPlan* plan, const mcfftDesc* descs, int co
     } else if (sl != p->info.scale_log2) {
       p->info.scale_log2 = 1;  // mixed scales: 1 flags "per transform"
     }
-    i = j;
   }
   if (r) {
     mcfftPlanDestroy(p);
@@ -1207,6 +1639,33 @@ mcfftResult mcfftPlanCreateBatch(mcfftPlan* plan, const mcfftDesc* descs, int co
     p->out_extent = std::max(p->out_extent, (descs[i].out_offset + len) * out_b);
   }
   return plan_finish(p, plan);
+}
+
+}  // namespace
+}  // namespace mcfft
+
+extern "C" {
+
+mcfftResult mcfftPlanCreateBatch(mcfftPlan* plan, const mcfftDesc* descs, int count,
+                                 mcfftPrecision precision, unsigned flags) {
+  if (!plan || !descs || count <= 0) return MCFFT_INVALID_VALUE;
+  for (int i = 0; i < count; ++i)
+    if (descs[i].ndim < 1 || descs[i].ndim > 3 || descs[i].batch < 1 || descs[i].in_offset < 0 ||
+        descs[i].out_offset < 0)
+      return MCFFT_INVALID_VALUE;
+  // Transforms of one shape form one group, wherever they lie (descriptors
+  // in any order); if that plan cannot run (an indexed group the batch
+  // kernel cannot take), groups of consecutive contiguous descriptors
+  // instead (MCFFT_GROUPING=adjacent forces that).
+  bool by_shape = true;
+  if (const char* e = std::getenv("MCFFT_GROUPING")) by_shape = std::strcmp(e, "adjacent") != 0;
+  if (by_shape) {
+    bool indexed = false;
+    const mcfftResult r = create_batch(plan, descs, count, precision, flags, true, &indexed);
+    if (r != MCFFT_UNSUPPORTED_SIZE || !indexed) return r;
+  }
+  bool unused = false;
+  return create_batch(plan, descs, count, precision, flags, false, &unused);
 }
 
 mcfftResult mcfftPlanCreate1d(mcfftPlan* plan, int64_t n, int64_t batch, mcfftPrecision precision,

@@ -50,6 +50,9 @@ bool fill_qpass(const TilePass& tp, int dir, const void* in, void* out, QPass* q
   q->col_blocks = a.col_blocks;
   q->in_tile_bytes = a.in_tile_bytes;
   q->variant = queue_variant(*tp.k);
+  q->l2_in = kL2Normal;
+  q->l2_out = kL2Normal;
+  q->aux = nullptr;
   q->wait_base = -1;
   q->sig_base = -1;
   q->sig_mul = 1;
@@ -65,26 +68,31 @@ const void* queue_fn(bool split) {
 }
 }  // namespace
 
-cudaError_t launch_queue(const QArgs& a, int grid, bool split, cudaStream_t st) {
-  const void* fn = queue_fn(split);
+cudaError_t launch_queue_fn(const void* fn, int smem_bytes, const QArgs& a, int grid,
+                            cudaStream_t st) {
   void* args[] = {const_cast<QArgs*>(&a)};
   // Cooperative: every CTA is resident, so a tile waiting for another
   // CTA's output never waits for a CTA that has not started.
-  return cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(17 * 32), args,
-                                     (size_t)QueueSmem::SMEM_BYTES, st);
+  return cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(17 * 32), args, (size_t)smem_bytes, st);
 }
 
-int queue_max_grid(int sms, bool split) {
+int queue_max_grid_fn(const void* fn, int smem_bytes, int sms) {
   int occ = 0;
-  const void* fn = queue_fn(split);
-  if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           QueueSmem::SMEM_BYTES) != cudaSuccess ||
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, 17 * 32, QueueSmem::SMEM_BYTES) !=
-          cudaSuccess) {
+  if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes) !=
+          cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, 17 * 32, smem_bytes) != cudaSuccess) {
     cudaGetLastError();
     return 0;
   }
   return occ * sms;
+}
+
+cudaError_t launch_queue(const QArgs& a, int grid, bool split, cudaStream_t st) {
+  return launch_queue_fn(queue_fn(split), QueueSmem::SMEM_BYTES, a, grid, st);
+}
+
+int queue_max_grid(int sms, bool split) {
+  return queue_max_grid_fn(queue_fn(split), QueueSmem::SMEM_BYTES, sms);
 }
 
 }  // namespace mcfft

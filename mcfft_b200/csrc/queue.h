@@ -18,4 +18,18 @@ cudaError_t launch_queue(const QArgs& a, int grid, bool split, cudaStream_t st);
 // sets the kernel's shared-memory limit.
 int queue_max_grid(int sms, bool split);
 
+// A fused four-step kernel (both passes of one 1D transform group in one
+// launch) for passes on tile variants v1 (with the four-step twiddle) and v2.
+struct FusedKernel {
+  bool split;
+  int v1, v2;
+  const void* fn;
+  int smem_bytes;
+};
+const FusedKernel* find_fused(bool split, int v1, int v2);
+// The same launch and occupancy query for any kernel over a QArgs block.
+cudaError_t launch_queue_fn(const void* fn, int smem_bytes, const QArgs& a, int grid,
+                            cudaStream_t st);
+int queue_max_grid_fn(const void* fn, int smem_bytes, int sms);
+
 }  // namespace mcfft

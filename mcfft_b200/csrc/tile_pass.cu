@@ -111,11 +111,13 @@ const TileKernel* find_tile_kernel(int L, bool posttw, bool split, int tile_poin
 
 bool tile_layout(layout::PassLayout* out, int L, int R, int C, layout::Kind ik, layout::Kind ok,
                  int in_elem, int out_elem, int64_t isp, int64_t isc, int64_t iso, int64_t osp,
-                 int64_t osc, int64_t oso, int64_t ncols, int64_t nouter, std::string* err) {
+                 int64_t osc, int64_t oso, int64_t ncols, int64_t nouter, std::string* err,
+                 int unsw) {
   char key[512];
-  snprintf(key, sizeof key, "%d %d %d %d %d %d %d %lld %lld %lld %lld %lld %lld %lld %lld", L, R,
-           C, (int)ik, (int)ok, in_elem, out_elem, (long long)isp, (long long)isc, (long long)iso,
-           (long long)osp, (long long)osc, (long long)oso, (long long)ncols, (long long)nouter);
+  snprintf(key, sizeof key, "%d %d %d %d %d %d %d %lld %lld %lld %lld %lld %lld %lld %lld %d", L,
+           R, C, (int)ik, (int)ok, in_elem, out_elem, (long long)isp, (long long)isc,
+           (long long)iso, (long long)osp, (long long)osc, (long long)oso, (long long)ncols,
+           (long long)nouter, unsw);
   {
     std::lock_guard<std::mutex> lk(g_lay_mu);
     auto it = g_lay_cache.find(key);
@@ -125,7 +127,7 @@ bool tile_layout(layout::PassLayout* out, int L, int R, int C, layout::Kind ik, 
     }
   }
   if (!layout::build(out, L, R, C, ik, ok, in_elem, out_elem, isp, isc, iso, osp, osc, oso, ncols,
-                     nouter, err))
+                     nouter, err, unsw))
     return false;
   // The kernels size their table reads at compile time (TileShape): items,
   // epilogue rows and stages must be exactly what the layout holds.

@@ -39,9 +39,12 @@ struct TilePass {
 };
 
 const TileKernel* find_tile_kernel(int L, bool posttw, bool split, int tile_points, bool in16);
+// unsw: bit 0 / bit 1 -- input / output staging without TMA swizzle (filled
+// by row gathers, see layout::make_staging).
 bool tile_layout(layout::PassLayout* out, int L, int R, int C, layout::Kind ik, layout::Kind ok,
                  int in_elem, int out_elem, int64_t isp, int64_t isc, int64_t iso, int64_t osp,
-                 int64_t osc, int64_t oso, int64_t ncols, int64_t nouter, std::string* err);
+                 int64_t osc, int64_t oso, int64_t ncols, int64_t nouter, std::string* err,
+                 int unsw = 0);
 bool tile_check_encode(const layout::Staging& s, const void* probe);
 bool tile_encode(CUtensorMap* map, const layout::Staging& s, const void* base);
 void fill_tile_args(TilePass* tp);

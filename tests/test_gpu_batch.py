@@ -1,9 +1,11 @@
 """Uneven batches: many transforms of different lengths and dimensionality
 in one plan (mcfftPlanCreateBatch), run by the persistent batch kernel in
-one launch (plain form) or pass by pass (split form), each transform
-checked against the FP64 oracle.  Also the batch kernel forced onto
-single-shape plans (MCFFT_QUEUE=1), including the four-step 1D and 2D/3D
-dependency chains.
+one launch, each transform checked against the FP64 oracle -- with the
+transforms of one shape next to each other, and in any order (one
+descriptor per transform, shapes interleaved, input and output orders
+different: per-transform coordinate tables and row gathers).  Also the
+batch kernel forced onto single-shape plans (MCFFT_QUEUE=1), including the
+four-step 1D and 2D/3D dependency chains.
 
 Tolerances as in test_gpu_parity: plain rel-L2 <= 1e-3, split <= 2e-6.
 """
@@ -142,3 +144,53 @@ def test_queue_repeated_exec_and_inverse():
                 ref = oracle.fftnd(xr[io:io + n].reshape((1,) + tuple(shape)), shape, sign=direction)
                 rel, _ = compare(y[oo:oo + n], ref * 2.0 ** -int(np.log2(n)))
                 assert rel < PLAIN_TOL, (shape, direction, rel)
+
+
+def _scattered(shapes, seed):
+    """One descriptor per transform; the transforms lie in a seeded random
+    order in the input and in another in the output."""
+    items = [shape for shape, count in shapes for _ in range(count)]
+    rng = np.random.default_rng(seed)
+    sizes = [int(np.prod(sh)) for sh in items]
+
+    def place(order):
+        offs, off = [0] * len(items), 0
+        for i in order:
+            offs[i] = off
+            off += sizes[i]
+        return offs, off
+
+    ioffs, total = place(rng.permutation(len(items)))
+    ooffs, _ = place(rng.permutation(len(items)))
+    return [(sh, 1, io, oo) for sh, io, oo in zip(items, ioffs, ooffs)], total
+
+
+@pytest.mark.parametrize("prec,flags", [(mc.PREC_FP16, mc.FLAG_NONE),
+                                        (mc.PREC_SPLIT, mc.FLAG_INPUT_F16),
+                                        (mc.PREC_SPLIT, mc.FLAG_NONE)])
+@pytest.mark.parametrize("seed", [1, 2])
+def test_uneven_batch_any_order_one_launch(prec, flags, seed):
+    shapes = SHAPES + [((256,), 7), ((1024,), 5), ((128, 256), 2)]
+    descs, total = _scattered(shapes, seed)
+    xr, y, info = _run_batch(descs, total, prec, flags, seed=seed)
+    assert info.launches == 1, info.launches
+    plain = prec == mc.PREC_FP16
+    assert _check_each(descs, xr, y, plain) < (PLAIN_TOL if plain else SPLIT_TOL)
+
+
+def test_uneven_batch_any_order_3d_and_repeat():
+    """3D transforms interleaved with others (the middle pass's per-slab
+    table), executed twice (the counters and tables are reused)."""
+    shapes = [((32, 64, 128), 2), ((64, 32, 32), 3), ((4096,), 3), ((1 << 15,), 2)]
+    descs, total = _scattered(shapes, 5)
+    x = rand_complex((total,), seed=5)
+    xd = to_device(x, True)
+    out = torch.empty(total, dtype=torch.complex32, device="cuda")
+    with mc.Plan(descs=descs, precision=mc.PREC_FP16) as p:
+        assert p.info().launches == 1
+        for _ in range(2):
+            out.view(torch.uint8).fill_(0xFF)
+            p.exec_ptr(xd.data_ptr(), out.data_ptr(), mc.FORWARD, torch.cuda.current_stream().cuda_stream)
+            torch.cuda.synchronize()
+            p.check_status()
+            assert _check_each(descs, rounded(x, True), from_device(out), True) < PLAIN_TOL

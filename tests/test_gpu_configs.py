@@ -104,11 +104,12 @@ def test_c2_every_transform(form):
     ref = oracle.fft1d(xr)
     del xr
     seg = [i * n for i in range(batch + 1)]
-    res = _norms(y, form == "plain", ref, seg, [info.scale_log2] * batch)
+    # the plain form's output carries 2^scale_log2: undo it before comparing
+    res = _norms(y, form == "plain", ref, seg, [-info.scale_log2] * batch)
     rel, mx = _worst(res)
     assert rel < (PLAIN_TOL if form == "plain" else SPLIT_TOL), (rel, mx)
     # the GPU reduction agrees with the CPU one on a transform
-    rel0, _ = oracle.error_norms(from_device(y[:n]) * 2.0 ** info.scale_log2, ref[0])
+    rel0, _ = oracle.error_norms(from_device(y[:n]) * 2.0 ** -info.scale_log2, ref[0])
     assert abs(rel0 - res[0]["rel_l2"]) <= 1e-9 * rel0
 
 
@@ -128,7 +129,7 @@ def test_c3_every_transform(form, variant):
         y, info = _exec(p, xd, f16)
     ref = oracle.fftnd(xr, list(dims))
     npt = int(np.prod(dims))
-    res = _norms(y, f16, ref, [i * npt for i in range(batch + 1)], [info.scale_log2] * batch)
+    res = _norms(y, f16, ref, [i * npt for i in range(batch + 1)], [-info.scale_log2] * batch)
     rel, mx = _worst(res)
     assert rel < (PLAIN_TOL if f16 else SPLIT_TOL), (rel, mx)
 
@@ -165,7 +166,7 @@ def test_c4_plain_forward():
     with mc.Plan(dims, 1, mc.PREC_FP16) as p:
         y, info = _exec(p, xd, True)
     ref = oracle.fftnd(xr, list(dims))
-    res = _norms(y, True, ref, [0, int(np.prod(dims))], [info.scale_log2])[0]
+    res = _norms(y, True, ref, [0, int(np.prod(dims))], [-info.scale_log2])[0]
     assert res["rel_l2"] < PLAIN_TOL, res
 
 
@@ -187,9 +188,10 @@ def _uneven_ref(shapes, offs, xr):
     return ref
 
 
+@pytest.mark.parametrize("order", ["draw", "sorted"])
 @pytest.mark.parametrize("form", ["plain", "split"])
-def test_c5_every_transform(form):
-    shapes, offs, total = W.uneven_layout("sorted")
+def test_c5_every_transform(form, order):
+    shapes, offs, total = W.uneven_layout(order)
     x = W.uneven_input(total)
     xr = rounded(x, True)
     xd = to_device(x, True)
@@ -203,7 +205,7 @@ def test_c5_every_transform(form):
         assert info.launches == 1
     ref = _uneven_ref(shapes, offs, xr)
     seg = offs + [total]
-    scales = [-int(np.log2(np.prod(s))) if form == "plain" else 0 for s in shapes]
+    scales = [int(np.log2(np.prod(s))) if form == "plain" else 0 for s in shapes]
     res = _norms(y, form == "plain", ref, seg, scales)
     rel, mx = _worst(res)
     assert rel < (PLAIN_TOL if form == "plain" else SPLIT_TOL), (rel, mx)

@@ -1,7 +1,8 @@
 """The plan builder's size limits, at the limits.
 
 The largest transforms a plan accepts run against the FP64 oracle in both
-forms: 1D 2^26 (the four-step pair of passes of 8192 points each), 2D
+forms: 1D 2^26 (the four-step pair of passes of 8192 points each), 1D 2^27
+(three passes of 512 points: the reference's largest 1D size), 2D
 8192 x 8192, and a 3D side of 8192 on each axis in turn.  The first sizes
 past the limits, and sizes that are not powers of two or are below 16, are
 refused with MCFFT_UNSUPPORTED_SIZE (an error, never a fallback).
@@ -26,7 +27,7 @@ from tests.gpu_util import compare, rand_complex, rounded, run  # noqa: E402
 PLAIN_TOL = 1e-3
 SPLIT_TOL = 2e-6
 
-BIG = [(1 << 26,), (8192, 8192)]
+BIG = [(1 << 26,), (1 << 27,), (8192, 8192)]
 SIDES_3D = [(8192, 16, 16), (16, 8192, 16), (16, 16, 8192)]
 
 _refs = {}
@@ -57,7 +58,7 @@ def test_largest_accepted_sizes(shape, prec):
         assert rel < SPLIT_TOL, (rel, mx)
 
 
-@pytest.mark.parametrize("shape", [(1 << 27,), (16384, 16), (16, 16384), (16384, 16, 16),
+@pytest.mark.parametrize("shape", [(1 << 28,), (16384, 16), (16, 16384), (16384, 16, 16),
                                    (16, 16, 16384), (8,), (16, 8), (3000,), (1 << 20 | 16,),
                                    (48, 64)])
 @pytest.mark.parametrize("prec", [mc.PREC_FP16, mc.PREC_SPLIT])
@@ -65,3 +66,19 @@ def test_sizes_past_the_limits_refused(shape, prec):
     with pytest.raises(mc.McfftError) as ei:
         mc.Plan(shape, 1, prec)
     assert ei.value.code == mc.UNSUPPORTED_SIZE
+
+
+@pytest.mark.parametrize("n,batch", [(1 << 16, 3), (1 << 18, 5), (1 << 21, 2)])
+@pytest.mark.parametrize("prec", [mc.PREC_FP16, mc.PREC_SPLIT])
+def test_three_pass_plan_at_smaller_sizes(n, batch, prec, monkeypatch):
+    """The three-pass 1D plan (taken for 2^27) forced at sizes with several
+    transforms: its last pass runs once per transform."""
+    monkeypatch.setenv("MCFFT_THREE_PASS", "1")
+    x = rand_complex((batch, n), seed=n % 997 + batch)
+    f16 = prec == mc.PREC_FP16
+    with mc.Plan((n,), batch, prec) as p:
+        assert p.info().num_passes == 2 + batch
+        y, sl = run(p, x, f16)
+    ref = oracle.fft1d(rounded(x, f16)) * 2.0 ** sl
+    rel, mx = compare(y, ref)
+    assert rel < (PLAIN_TOL if f16 else SPLIT_TOL), (rel, mx)
