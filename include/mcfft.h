@@ -97,6 +97,10 @@ typedef struct {
   int num_descs;           /* transform groups (mcfftPlanCreateBatch) */
   int launches;            /* this library's kernel launches per exec (1: batch queue) */
   int timed_passes;        /* passes the plan-time tuner timed (0: all from wisdom or untuned) */
+  /* Added in 0.2.0 (the struct grew at its end). */
+  int64_t fourstep_n1;     /* first group, 1D four-step: the chosen n1 of n = n1 * n2; else 0 */
+  int tile_points;         /* points per tile of the first pass (0: direct-load kernel) */
+  int ctas;                /* CTAs of the first launch */
 } mcfftPlanInfo;
 
 MCFFT_API mcfftResult mcfftPlanCreate1d(mcfftPlan* plan, int64_t n, int64_t batch,

@@ -61,7 +61,9 @@ class PlanInfo(ctypes.Structure):
                 ("scale_log2", ctypes.c_int), ("elements", ctypes.c_int64),
                 ("in_bytes", ctypes.c_int64), ("out_bytes", ctypes.c_int64),
                 ("workspace_bytes", ctypes.c_int64), ("num_descs", ctypes.c_int),
-                ("launches", ctypes.c_int), ("timed_passes", ctypes.c_int)]
+                ("launches", ctypes.c_int), ("timed_passes", ctypes.c_int),
+                ("fourstep_n1", ctypes.c_int64), ("tile_points", ctypes.c_int),
+                ("ctas", ctypes.c_int)]
 
 
 _lib = None

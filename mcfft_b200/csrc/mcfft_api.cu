@@ -43,7 +43,7 @@
 namespace mcfft {
 namespace {
 
-constexpr int kVersion = 100;  // 0.1.0
+constexpr int kVersion = 200;  // 0.2.0
 
 enum Buf { kUserIn = 0, kUserOut = 1, kScratch = 2 };
 
@@ -146,6 +146,8 @@ struct mcfftPlan_st {
   // An indexed transform group (per-transform offsets), which only the
   // batch queue can run.
   bool indexed = false;
+  // Four-step split n1 = 2^fs_lg1 of the 1D group being built (0: default).
+  int fs_lg1 = 0;
   // Executable graphs of recent execs, keyed by (in, out, direction): an
   // exec repeated on the same buffers replays its captured launches.
   struct GraphEntry {
@@ -807,6 +809,7 @@ mcfftResult build_group_passes(mcfftPlan p, int ndim, const int64_t* dims, int64
     const int lg = ilog2(n);
     int lg1 = lg / 2;
     if (const char* e = std::getenv("MCFFT_FOURSTEP_N1")) lg1 = ilog2(std::atoll(e));
+    if (p->fs_lg1 > 0) lg1 = p->fs_lg1;  // the plan-time tuner's choice or candidate
     const int64_t n1 = int64_t(1) << lg1, n2 = n >> lg1;
     if (n1 < 16 || n2 < 16 || n1 > kMaxSinglePass || n2 > kMaxSinglePass)
       return MCFFT_UNSUPPORTED_SIZE;
@@ -944,10 +947,92 @@ void link_group(mcfftPlan p, size_t first, int ndim, const int64_t* dims, int64_
   }
 }
 
+// Plan-time tuning of a 1D four-step group's split n = n1 * n2: besides
+// the default n1 = 2^floor(lg n / 2), the neighbouring splits (n1 / 2,
+// 2 n1) whose passes both run on the TMA-fed kernels are built and timed
+// on scratch buffers (each pass's median CUDA-event time, summed); the
+// fastest split wins when it is faster than the default by more than 3 %.
+// The choice is recorded as wisdom ("fourstep" records) and reported in
+// mcfftPlanInfo.fourstep_n1.  MCFFT_AUTOTUNE=0 or MCFFT_FOURSTEP_N1 keeps
+// the default (or the forced split).
+int tune_fourstep(mcfftPlan p, int64_t n, int64_t batch, int64_t in_off, int64_t out_off) {
+  const int lg = ilog2(n), def = lg / 2;
+  if (n <= (p->split ? kMaxTilePass / 2 : kMaxTilePass) || n > kMaxSinglePass * kMaxSinglePass)
+    return 0;
+  if (std::getenv("MCFFT_FOURSTEP_N1") || std::getenv("MCFFT_THREE_PASS")) return 0;
+  if (const char* e = std::getenv("MCFFT_AUTOTUNE"))
+    if (std::atoi(e) == 0) return 0;
+  char kb[160];
+  std::snprintf(kb, sizeof kb, "fourstep n%lld b%lld p%d f%u", (long long)n, (long long)batch,
+                (int)p->prec, p->flags);
+  const std::string key = gpu_key(p) + "\t" + kb;
+  if (const int rec = wisdom_find(key)) return rec;
+  // each candidate's passes are built, timed, then removed again
+  const size_t first = p->passes.size();
+  const size_t scratch0 = p->scratch_bytes;
+  const size_t eb = p->split ? 8 : 4;
+  void *a = nullptr, *b = nullptr, *c = nullptr;
+  const size_t bytes = (size_t)n * batch * eb;
+  if (cudaMalloc(&a, bytes) != cudaSuccess || cudaMalloc(&b, bytes) != cudaSuccess ||
+      cudaMalloc(&c, bytes) != cudaSuccess || cudaMemset(a, 0, bytes) != cudaSuccess ||
+      cudaMemset(b, 0, bytes) != cudaSuccess || cudaMemset(c, 0, bytes) != cudaSuccess) {
+    cudaGetLastError();
+    if (a) cudaFree(a);
+    if (b) cudaFree(b);
+    if (c) cudaFree(c);
+    return 0;
+  }
+  float best_t = -1.f, def_t = -1.f;
+  int best = def;
+  for (int lg1 : {def, def - 1, def + 1}) {
+    const int64_t n1 = int64_t(1) << lg1, n2 = n >> lg1;
+    if (n1 < 32 || n2 < 32 || n1 > kMaxTilePass || n2 > kMaxTilePass) continue;
+    p->fs_lg1 = lg1;
+    int sl = 0;
+    const mcfftResult r = build_group_passes(p, 1, &n, batch, in_off, out_off, &sl);
+    float t = 0.f;
+    bool ok = r == MCFFT_SUCCESS && p->passes.size() == first + 2;
+    for (size_t i = first; ok && i < p->passes.size(); ++i) {
+      const Pass& ps = p->passes[i];
+      if (!ps.tiled) {
+        ok = false;
+        break;
+      }
+      // pass 1 reads a and writes the scratch c; pass 2 reads c and writes b
+      const float ti = time_tile_pass(ps.tp, i == first ? a : c, i == first ? c : b, 0);
+      if (ti <= 0.f) ok = false;
+      t += ti;
+    }
+    p->passes.resize(first);
+    p->scratch_bytes = scratch0;
+    p->fs_lg1 = 0;
+    if (!ok) continue;
+    ++p->info.timed_passes;
+    if (std::getenv("MCFFT_DEBUG_PLAN"))
+      fprintf(stderr, "[mcfft] tune four-step n=%lld: n1=%lld %.4f ms\n", (long long)n,
+              (long long)n1, t);
+    if (lg1 == def) def_t = t;
+    if (best_t < 0.f || t < best_t) {
+      best_t = t;
+      best = lg1;
+    }
+  }
+  cudaFree(a);
+  cudaFree(b);
+  cudaFree(c);
+  if (def_t > 0.f && best != def && best_t >= 0.97f * def_t) best = def;
+  if (def_t > 0.f) wisdom_put(key, best);
+  return best;
+}
+
 mcfftResult build_group(mcfftPlan p, int ndim, const int64_t* dims, int64_t batch,
                         int64_t in_off, int64_t out_off, int* scale_log2) {
   const size_t first = p->passes.size();
+  p->fs_lg1 = ndim == 1 ? tune_fourstep(p, dims[0], batch, in_off, out_off) : 0;
   mcfftResult r = build_group_passes(p, ndim, dims, batch, in_off, out_off, scale_log2);
+  if (!r && ndim == 1 && first == 0 && p->passes.size() == 2)
+    p->info.fourstep_n1 = p->passes[0].spec.L;
+  p->fs_lg1 = 0;
   int64_t points = batch;
   for (int d = 0; d < ndim; ++d) points *= dims[d];
   if (!r) r = autotune_group(p, first, points);
@@ -1059,20 +1144,6 @@ mcfftResult build_indexed_group(mcfftPlan p, int ndim, const int64_t* dims,
   return MCFFT_SUCCESS;
 }
 
-// Builds the batch queue (every pass of the plan in one persistent launch)
-// for plans of several transform groups (uneven batches) -- or any plan
-// with MCFFT_QUEUE=1; MCFFT_QUEUE=0 disables it -- when every pass runs on
-// a tile-kernel variant the batch kernel holds and the passes fit its
-// parameter block; otherwise the plan launches pass by pass (one transform
-// shape is faster that way: each pass kernel keeps its tables in its
-// parameter block).
-// Queue order (queue_order.h): first passes in chunks of QC (sixteen) tiles
-// per CTA, group after group; after each chunk, every later-pass tile whose
-// key was completed at least QC tiles per CTA earlier, across all groups.
-// Every dependency points backwards, a CTA runs several tiles of one pass in
-// a row (its tables stay in shared memory), and the tail of one group's
-// later pass runs beside the next group's first pass instead of waiting on
-// the tiles queued just before it.
 // L2 use of pass i in the batch kernels (MCFFT_L2_HINTS=1; off by default:
 // measured slower on the four-step pair, whose column tiles read half
 // lines that the neighbouring tile reads again): an intermediate another
@@ -1145,14 +1216,15 @@ QPassAux make_aux(mcfftPlan p, size_t i, bool* any) {
   return x;
 }
 
-// A single 1D four-step transform group whose pair of tile variants has a
-// fused kernel runs both passes in one launch of it (MCFFT_FUSED=0: pass by
-// pass), its items ordered in chunks of two tiles per CTA (a transform's
-// second pass follows its first within a few tiles per CTA, while its
-// intermediate is still in L2).
+// With MCFFT_FUSED=1, a single 1D four-step transform group whose pair of
+// tile variants has a fused kernel runs both passes in one launch of it,
+// its items ordered in chunks of two tiles per CTA (a transform's second
+// pass follows its first within a few tiles per CTA, while its
+// intermediate is still in L2).  Off by default: on the 2^20 x 64 workload
+// the two pass launches measured faster (0.258 against 0.294 ms).
 const FusedKernel* fused_for(mcfftPlan p) {
-  if (const char* e = std::getenv("MCFFT_FUSED"))
-    if (std::atoi(e) == 0) return nullptr;
+  const char* e = std::getenv("MCFFT_FUSED");
+  if (!e || std::atoi(e) == 0) return nullptr;
   if (p->ngroups != 1 || p->passes.size() != 2 || p->no_queue) return nullptr;
   const Pass &a = p->passes[0], &b = p->passes[1];
   if (!a.tiled || !b.tiled || !a.spec.posttw || b.spec.posttw || a.out_buf != kScratch ||
@@ -1163,6 +1235,20 @@ const FusedKernel* fused_for(mcfftPlan p) {
   return find_fused(p->split, v1, v2);
 }
 
+// Builds the batch queue (every pass of the plan in one persistent launch)
+// for plans of several transform groups (uneven batches) -- or any plan
+// with MCFFT_QUEUE=1; MCFFT_QUEUE=0 disables it -- when every pass runs on
+// a tile-kernel variant the batch kernel holds and the passes fit its
+// parameter block; otherwise the plan launches pass by pass (one transform
+// shape is faster that way: each pass kernel keeps its tables in its
+// parameter block).
+// Queue order (queue_order.h): first passes in chunks of QC (sixteen) tiles
+// per CTA, group after group; after each chunk, every later-pass tile whose
+// key was completed at least QC tiles per CTA earlier, across all groups.
+// Every dependency points backwards, a CTA runs several tiles of one pass in
+// a row (its tables stay in shared memory), and the tail of one group's
+// later pass runs beside the next group's first pass instead of waiting on
+// the tiles queued just before it.
 mcfftResult build_queue(mcfftPlan p) {
   const FusedKernel* fk = fused_for(p);
   bool want = p->ngroups > 1 || fk || p->indexed;
@@ -1303,6 +1389,11 @@ mcfftResult plan_finish(mcfftPlan p, mcfftPlan* out) {
   }
   p->info.num_passes = (int)p->passes.size();
   p->info.launches = p->q.on ? 1 : (int)p->passes.size();
+  if (!p->passes.empty()) {
+    const Pass& f = p->passes[0];
+    p->info.tile_points = f.tiled ? f.tp.k->tile_points : 0;
+    p->info.ctas = p->q.on ? p->q.grid : (f.tiled ? f.tp.grid : f.grid);
+  }
   p->info.workspace_bytes = (int64_t)p->scratch_bytes;
   *out = p;
   return MCFFT_SUCCESS;
@@ -1792,7 +1883,12 @@ mcfftResult mcfftWisdomImport(const char* path) {
     const std::string v = l.substr(t3 + 1);
     char* end = nullptr;
     const long tp = std::strtol(v.c_str(), &end, 10);
-    if (v.empty() || *end || (tp != 8192 && tp != 16384)) { ok = false; break; }
+    // tile-shape records hold 8192 or 16384 points; four-step records lg n1
+    const bool fs = l.find("\tfourstep ") != std::string::npos;
+    if (v.empty() || *end || (fs ? (tp < 4 || tp > 13) : (tp != 8192 && tp != 16384))) {
+      ok = false;
+      break;
+    }
     got.push_back({l.substr(0, t3), (int)tp});
   }
   std::fclose(f);

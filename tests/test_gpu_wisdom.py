@@ -1,7 +1,9 @@
-"""Autotuning records on the GPU: a plan's tuner times its tiled passes and
-records the choices; after export, forget and import, a new plan of the same
-shape takes the recorded shapes without timing and computes bit-identical
-results."""
+"""Autotuning on the GPU: a plan's tuner times its four-step split and its
+tiled passes' tile shapes and records the choices; after export, forget and
+import, a new plan of the same shape takes the recorded choices without
+timing and computes bit-identical results.  Non-default four-step splits
+(the tuner's other candidates) stay within the forms' tolerances and are
+reported by mcfftPlanInfo."""
 import numpy as np
 import pytest
 
@@ -12,7 +14,8 @@ if not torch.cuda.is_available():
     pytest.skip("no CUDA device", allow_module_level=True)
 
 import mcfft_b200 as mc  # noqa: E402
-from tests.gpu_util import rand_complex, run  # noqa: E402
+from oracle import oracle  # noqa: E402
+from tests.gpu_util import compare, rand_complex, rounded, run  # noqa: E402
 
 
 def test_wisdom_skips_timing_and_keeps_results(tmp_path):
@@ -22,15 +25,20 @@ def test_wisdom_skips_timing_and_keeps_results(tmp_path):
     try:
         with mc.Plan((n,), batch, mc.PREC_FP16) as p:
             info = p.info()
-            assert info.timed_passes == info.num_passes == 2
+            # three four-step splits, then the chosen split's two passes
+            assert info.timed_passes == 3 + info.num_passes, info.timed_passes
+            assert info.fourstep_n1 in (512, 1024, 2048), info.fourstep_n1
+            assert info.tile_points in (8192, 16384) and info.ctas > 0
+            timed = info.timed_passes
             y1, _ = run(p, x, True)
         with mc.Plan((n,), batch, mc.PREC_FP16) as p:
             assert p.info().timed_passes == 0  # records of this process
         path = str(tmp_path / "wisdom.txt")
         mc.wisdom_export(path)
+        assert "fourstep n1048576" in open(path).read()
         mc.wisdom_forget()
         with mc.Plan((n,), batch, mc.PREC_FP16) as p:
-            assert p.info().timed_passes == 2  # forgotten: timed again
+            assert p.info().timed_passes == timed  # forgotten: timed again
         mc.wisdom_forget()
         mc.wisdom_import(path)
         with mc.Plan((n,), batch, mc.PREC_FP16) as p:
@@ -39,3 +47,20 @@ def test_wisdom_skips_timing_and_keeps_results(tmp_path):
         assert np.array_equal(y1, y2)
     finally:
         mc.wisdom_forget()
+
+
+@pytest.mark.parametrize("prec", [mc.PREC_FP16, mc.PREC_SPLIT])
+@pytest.mark.parametrize("n1", [256, 512, 2048, 4096])
+def test_non_default_fourstep_splits(prec, n1, monkeypatch):
+    n, batch = 1 << 20, 2
+    if prec == mc.PREC_SPLIT and n1 > 2048:
+        pytest.skip("split tiles hold at most 2048 points per transform")
+    monkeypatch.setenv("MCFFT_FOURSTEP_N1", str(n1))
+    x = rand_complex((batch, n), seed=n1)
+    f16 = prec == mc.PREC_FP16
+    with mc.Plan((n,), batch, prec) as p:
+        assert p.info().fourstep_n1 == n1
+        y, sl = run(p, x, f16)
+    ref = oracle.fft1d(rounded(x, f16)) * 2.0 ** sl
+    rel, _ = compare(y, ref)
+    assert rel < (1e-3 if f16 else 2e-6), rel
