@@ -194,13 +194,14 @@ struct Variant {
 __device__ __forceinline__ void discard_tile(const QPassAux& X, int64_t col_blocks, int64_t t,
                                              int ctid, int nct) {
   const int64_t cb = t % col_blocks, outer = t / col_blocks;
-  const uint32_t per_row = X.disc_row_bytes >> 7;
-  const uint32_t lines = per_row * (uint32_t)X.disc_C;
+  // rows hold a power of two of 128-byte lines: line i of the tile is line
+  // i & (per_row - 1) of row i >> lg
+  const uint32_t lg = (uint32_t)(__ffs(X.disc_row_bytes) - 8);
+  const uint32_t lines = (uint32_t)X.disc_C << lg;
   const char* base = X.disc_base + outer * X.disc_so + cb * X.disc_C * X.disc_sc;
-  for (uint32_t i = (uint32_t)ctid; i < lines; i += (uint32_t)nct) {
-    const uint32_t r = i / per_row, l = i - r * per_row;
-    tile::discard_l2_line(base + r * X.disc_sc + ((int64_t)l << 7));
-  }
+  for (uint32_t i = (uint32_t)ctid; i < lines; i += (uint32_t)nct)
+    tile::discard_l2_line(base + (int64_t)(i >> lg) * X.disc_sc +
+                          ((int64_t)(i & ((1u << lg) - 1u)) << 7));
 }
 
 // RESIDENT: the pass's tables are already in shared memory (x points at
@@ -355,7 +356,17 @@ __device__ __forceinline__ void producer_loop(const QArgs& a, uint32_t sS0, uint
     }
     if (moved) {
       idle = false;
+    } else if (is < il && (il == is + 2 || il == nlocal || *abort_flag)) {
+      // Only the consumers' release of tile `is` can make progress: wait for
+      // it on the barrier (a bounded try-wait suspends the thread instead of
+      // spinning, which would take issue slots from the consumers).
+      if (!sm100::mbar_wait_bounded(&outrdy[is & 1], (uint32_t)(is >> 1) & 1u, kWaitLimit) ||
+          *abort_flag) {
+        *abort_flag = 1;
+        break;
+      }
     } else {
+      // Waiting for a dependency (or for both events): poll with a back-off.
       const uint32_t now = sm100::globaltimer_ns();
       if (!idle) {
         idle = true;
@@ -365,7 +376,7 @@ __device__ __forceinline__ void producer_loop(const QArgs& a, uint32_t sS0, uint
         *abort_flag = 1;
         break;
       }
-      __nanosleep(32);
+      __nanosleep(128);
     }
   }
   if (sig >= 0) signal(sig);
