@@ -484,7 +484,13 @@ mcfftResult add_tile_pass(mcfftPlan p, const PassSpec& s, int only_tile_points =
     }
     a.post_mask = (uint64_t)s.postN - 1;
     a.post_shift = (uint32_t)sh;
-    a.post_scale = s.postN <= (int64_t(1) << 24) ? (float)(2.0 / (double)s.postN) : 0.f;
+    // W_N^e from the exact angle e (2 / N) (sine / cosine in the kernel) up to
+    // N = 2^24, else from the FP64-generated two-level table;
+    // MCFFT_FOURSTEP_TABLES=1 takes the tables for every N (to measure the
+    // angle path's error against them)
+    const char* ft = std::getenv("MCFFT_FOURSTEP_TABLES");
+    const bool tables = (ft && std::atoi(ft) != 0) || s.postN > (int64_t(1) << 24);
+    a.post_scale = tables ? 0.f : (float)(2.0 / (double)s.postN);
   }
   for (int dir = 0; dir < 2; ++dir) {
     tp.bmat[dir] = p->bsw64[dir];
@@ -1302,7 +1308,9 @@ mcfftResult build_queue(mcfftPlan p) {
     qo[i].keys = ps.level > 0 ? ps.keys : 0;
     qo[i].grp = ps.grp;
   }
-  const std::vector<QOrderItem> order = queue_order(qo, G, QC);
+  int64_t QLAG = 0;  // lag between a key's completion and its readers (0: QC)
+  if (const char* e = std::getenv("MCFFT_QUEUE_LAG")) QLAG = std::max<int64_t>(0, std::atoll(e));
+  const std::vector<QOrderItem> order = queue_order(qo, G, QC, QLAG);
   if (order.empty()) return MCFFT_SUCCESS;  // no consistent order: pass by pass
   std::vector<QItem> items(order.size());
   for (size_t i = 0; i < order.size(); ++i) items[i] = {order[i].pass, order[i].tile};

@@ -42,8 +42,10 @@ struct QOrderItem {
 
 // Returns the items in queue order, or an empty vector if the passes do not
 // describe a consistent dependency chain (then the plan runs pass by pass).
+// QLAG (0: QC) sets the lag, in tiles per CTA, between a key's completion
+// and its dependent tiles separately from the chunk size.
 inline std::vector<QOrderItem> queue_order(const std::vector<QOrderPass>& ps, int64_t G,
-                                           int64_t QC) {
+                                           int64_t QC, int64_t QLAG = 0) {
   struct Grp {
     size_t first = 0;
     int nl = 0;
@@ -69,7 +71,7 @@ inline std::vector<QOrderItem> queue_order(const std::vector<QOrderPass>& ps, in
     }
     i = j;
   }
-  const int64_t lag = std::max<int64_t>(1, QC * G);
+  const int64_t lag = std::max<int64_t>(1, (QLAG > 0 ? QLAG : QC) * G);
   std::vector<QOrderItem> out;
   out.reserve((size_t)total);
   auto emit = [&](Grp& g, int l) {

@@ -161,3 +161,18 @@ def test_plain_8k_tiles(shape, batch, monkeypatch):
     ref = oracle.fftnd(rounded(x, True), shape) * 2.0 ** sl
     rel, mx = compare(y, ref)
     assert rel < PLAIN_TOL, (rel, mx)
+
+
+@pytest.mark.parametrize("prec", [mc.PREC_FP16, mc.PREC_SPLIT])
+def test_fourstep_twiddle_tables_switch(prec, monkeypatch):
+    """The four-step twiddles from FP64-generated tables instead of the
+    sine / cosine of the exact angle (MCFFT_FOURSTEP_TABLES=1): same bounds."""
+    monkeypatch.setenv("MCFFT_FOURSTEP_TABLES", "1")
+    n, batch = 1 << 20, 2
+    x = rand_complex((batch, n), seed=77)
+    f16 = prec == mc.PREC_FP16
+    with mc.Plan((n,), batch, prec) as p:
+        y, sl = run(p, x, f16)
+    ref = oracle.fft1d(rounded(x, f16)) * 2.0 ** sl
+    rel, _ = compare(y, ref)
+    assert rel < (PLAIN_TOL if f16 else SPLIT_TOL), rel
