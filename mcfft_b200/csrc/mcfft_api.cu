@@ -1685,6 +1685,13 @@ mcfftResult create_batch(mcfftPlan* plan, const mcfftDesc* descs, int count,
         g->out.push_back(d.out_offset + b * n);
       }
     }
+    // groups are independent: queue them by dimensionality, then shape
+    std::stable_sort(groups.begin(), groups.end(), [](const Group& a, const Group& b) {
+      if (a.shape.ndim != b.shape.ndim) return a.shape.ndim < b.shape.ndim;
+      for (int k = 0; k < a.shape.ndim; ++k)
+        if (a.shape.dims[k] != b.shape.dims[k]) return a.shape.dims[k] < b.shape.dims[k];
+      return false;
+    });
   } else {
     for (int i = 0; i < count;) {
       mcfftDesc g = descs[i];
