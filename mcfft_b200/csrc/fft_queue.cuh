@@ -188,6 +188,19 @@ struct Variant {
 // with tile routine TL; returns the local index of the first item of
 // another pass.  The pass's tables go to shared memory and its layout
 // entries to registers once per run.
+// The (pass, tile) of the item in staging buffer b, written by the producer
+// before it arms that buffer's load barrier (its arrive releases the write;
+// the consumers' wait on the barrier acquires it), so that the consumers
+// never read the item list in global memory.  Two 8-byte slots after the
+// other barrier-area words.
+__device__ __forceinline__ volatile QItem* item_ring(uint64_t* full) {
+  return reinterpret_cast<volatile QItem*>(full + 4 + 20);
+}
+__device__ __forceinline__ QItem ring_item(uint64_t* full, int b) {
+  volatile QItem* r = item_ring(full);
+  return QItem{r[b].pass, r[b].tile};
+}
+
 // Drops the source lines of tile t of a pass whose input is read for the
 // last time (QPassAux::disc_base); the consumer threads share the lines.
 // Runs once the tile's load has completed.
@@ -214,7 +227,6 @@ __device__ __forceinline__ int64_t run_items(const QArgs& a, uint32_t pi, const 
   static_assert(RESIDENT || !TL::T::TW_SMEM || TL::T::TW_ROWS * 128 <= QueueSmem::TWS_BYTES,
                 "stage rows");
   const QPass& P = a.pass[pi];
-  const int64_t G = gridDim.x;
   if constexpr (!RESIDENT) {
     // every consumer is past the previous tile's last barrier, so nobody
     // still reads the old tables
@@ -227,10 +239,11 @@ __device__ __forceinline__ int64_t run_items(const QArgs& a, uint32_t pi, const 
   volatile int* abort_flag;
   if constexpr (SPLIT) abort_flag = x.t.abort_flag;
   else abort_flag = x.abort_flag;
+  const bool disc = P.aux && P.aux->disc_base;
   for (;;) {
     const int b = (int)(k & 1);
-    const int64_t t = a.items[blockIdx.x + k * G].tile;
-    if (P.aux && P.aux->disc_base) discard_tile(*P.aux, P.col_blocks, t, ctid, TL::NCT);
+    const int64_t t = ring_item(full, b).tile;  // the tile in buffer b (loaded: full[b] waited)
+    if (disc) discard_tile(*P.aux, P.col_blocks, t, ctid, TL::NCT);
     if constexpr (SPLIT) {
       TL::run(P, x, ctid, b, t % P.col_blocks, k, mphase, ient, eent);
     } else {
@@ -238,12 +251,15 @@ __device__ __forceinline__ int64_t run_items(const QArgs& a, uint32_t pi, const 
     }
     if (*abort_flag) return nlocal;
     if (ctid == 0) tile::mbar_arrive(&outrdy[b]);
-    if (++k >= nlocal || a.items[blockIdx.x + k * G].pass != pi) return k;
+    if (++k >= nlocal) return k;
+    // the next item's buffer: once it is loaded, its ring slot tells its pass
+    // (a run that ends here returns with that wait done; repeating it is free)
     if (!sm100::mbar_wait_bounded(&full[k & 1], (uint32_t)(k >> 1) & 1u, kWaitLimit)) {
       *abort_flag = 1;
       return nlocal;
     }
     if (*abort_flag) return nlocal;
+    if (ring_item(full, (int)(k & 1)).pass != pi) return k;
   }
 }
 
@@ -333,6 +349,9 @@ __device__ __forceinline__ void producer_loop(const QArgs& a, uint32_t sS0, uint
       if (ready) {
         const uint32_t dst = (il & 1) ? sS1 : sS0;
         const int64_t cb = it.tile % P.col_blocks;
+        volatile QItem* ring = item_ring(full);
+        ring[il & 1].pass = it.pass;
+        ring[il & 1].tile = it.tile;
         sm100::mbar_arrive_expect_tx(&full[il & 1], P.in_tile_bytes);
         const QPassAux* X = P.aux;
         if (X && X->in_gtab) {
@@ -479,7 +498,7 @@ __global__ void __maxnreg__(96) fft_queue(const __grid_constant__ QArgs a) {
     for (int64_t k = 0; k < nlocal;) {
       if (!sm100::mbar_wait_bounded(&full[k & 1], (uint32_t)(k >> 1) & 1u, kWaitLimit)) *abort_flag = 1;
       if (*abort_flag) break;
-      const uint32_t pi = a.items[blockIdx.x + k * G].pass;
+      const uint32_t pi = queue::ring_item(full, (int)(k & 1)).pass;
       if constexpr (SPLIT) {
         switch (a.pass[pi].variant) {
 #define MCFFT_QCASE(V)                                                                          \
@@ -638,7 +657,7 @@ __global__ void __maxnreg__(96) fft_fused(const __grid_constant__ QArgs a) {
     for (int64_t k = 0; k < nlocal;) {
       if (!sm100::mbar_wait_bounded(&full[k & 1], (uint32_t)(k >> 1) & 1u, kWaitLimit)) *abort_flag = 1;
       if (*abort_flag) break;
-      const uint32_t pi = a.items[blockIdx.x + k * G].pass;
+      const uint32_t pi = queue::ring_item(full, (int)(k & 1)).pass;
       if constexpr (SPLIT) {
         const SplitCtx s1{x1, base_u + F::OFF_B + 2048, red};
         const SplitCtx s2{x2, base_u + F::OFF_B + 2048, red};
