@@ -31,8 +31,10 @@
  *                     (scale_log2 = 0), like FFTW_FORWARD/FFTW_BACKWARD.
  *
  * Sizes: every dimension a power of two >= 16; 1D lengths up to 2^27 (one
- * pass up to 4096, split form 2048; a four-step pair of passes up to 2^26;
- * three passes for 2^27); 2D/3D sides up to 8192 (one pass per axis).
+ * pass up to 4096, split form 2048; past that a four-step pair of passes,
+ * or three passes from 2^24 points (split form 2^23) and for 2^27, the
+ * decomposition tuned at plan time); 2D/3D sides up to 8192 (one pass per
+ * axis).
  */
 #ifndef MCFFT_H_
 #define MCFFT_H_
@@ -98,7 +100,8 @@ typedef struct {
   int launches;            /* this library's kernel launches per exec (1: batch queue) */
   int timed_passes;        /* passes the plan-time tuner timed (0: all from wisdom or untuned) */
   /* Added in 0.2.0 (the struct grew at its end). */
-  int64_t fourstep_n1;     /* first group, 1D four-step: the chosen n1 of n = n1 * n2; else 0 */
+  int64_t fourstep_n1;     /* first group, 1D past one pass: the chosen n1 of n = n1 * n2
+                              (three passes, num_passes 3: of n = n1 * n2 * n3); else 0 */
   int tile_points;         /* points per tile of the first pass (0: direct-load kernel) */
   int ctas;                /* CTAs of the first launch */
 } mcfftPlanInfo;
@@ -194,7 +197,9 @@ MCFFT_API mcfftResult mcfftErrorNorms(const void* y, int y_f16, const void* ref,
 
 /* Autotuning records ("wisdom"; the reference has no tuner and no such
  * file).  Creating a plain-form plan times each pass's two tile shapes once
- * and records the faster per GPU model and pass; later plans in the process
+ * and records the faster per GPU model and pass; a 1D plan past one pass
+ * also times its decompositions (four-step splits n1 * n2 and, from 2^21
+ * points, three passes) and records the fastest; later plans in the process
  * reuse the record instead of timing.  Export writes this process's records
  * to a text file, Import reads such a file (adding to and replacing records;
  * a malformed file changes nothing and returns MCFFT_INVALID_VALUE), Forget

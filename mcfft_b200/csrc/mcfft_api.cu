@@ -742,6 +742,23 @@ constexpr int64_t kMaxTilePass = 4096;  // 1D lengths above run as four-step (sp
 
 constexpr int64_t kMaxLength1d = int64_t(1) << 27;
 
+// The three-pass decomposition as a choice of the four-step tuner (in
+// mcfftPlan_st::fs_lg1 and in "fourstep" wisdom records).
+constexpr int kThreePass = -1;
+
+// The untuned decomposition of a 1D length past one pass: the four-step
+// split n1 = 2^floor(lg n / 2), or three passes from 2^24 points (plain
+// form) and 2^23 (split form).  Measured on a B200, 2^26 points in all per
+// exec: the split form's tile kernels hold at most 2048 points per column,
+// so its four-step pairs past 2^22 run a direct-load pass (2^23: 1.44 ms
+// against 0.80 ms in three passes); the plain form's pair of 4096-point
+// passes at 2^24 takes 0.65 ms against 0.41 ms in three, and past 2^24 its
+// pairs run a direct-load pass (2^26: 2.68 ms against 0.42 ms).
+int default_lg1(const mcfftPlan p, int64_t n) {
+  if (n >= (p->split ? (int64_t(1) << 23) : (int64_t(1) << 24))) return kThreePass;
+  return ilog2(n) / 2;
+}
+
 // 1D lengths of 2^27 (the reference plans 2^27 in three passes,
 // source/mcfft_1d_device.cpp:762-771): n = n1 * n2 * n3, m = n2 * n3, the
 // four-step split applied twice --
@@ -809,13 +826,14 @@ mcfftResult build_group_passes(mcfftPlan p, int ndim, const int64_t* dims, int64
     }
     // MCFFT_THREE_PASS=1 takes the three-pass plan for every length past one
     // pass (a test switch: the same code path at sizes that test quickly)
+    // MCFFT_FOURSTEP_N1 forces a four-step split
     const char* three = std::getenv("MCFFT_THREE_PASS");
-    if (n > kMaxSinglePass * kMaxSinglePass || (three && std::atoi(three) != 0 && n >= 4096 * 16))
-      return build_three_pass(p, n, batch, in_off, out_off);
-    const int lg = ilog2(n);
-    int lg1 = lg / 2;
+    int lg1 = default_lg1(p, n);
     if (const char* e = std::getenv("MCFFT_FOURSTEP_N1")) lg1 = ilog2(std::atoll(e));
-    if (p->fs_lg1 > 0) lg1 = p->fs_lg1;  // the plan-time tuner's choice or candidate
+    if (p->fs_lg1 != 0) lg1 = p->fs_lg1;  // the plan-time tuner's choice or candidate
+    if (n > kMaxSinglePass * kMaxSinglePass || (three && std::atoi(three) != 0 && n >= 4096 * 16) ||
+        lg1 == kThreePass)
+      return build_three_pass(p, n, batch, in_off, out_off);
     const int64_t n1 = int64_t(1) << lg1, n2 = n >> lg1;
     if (n1 < 16 || n2 < 16 || n1 > kMaxSinglePass || n2 > kMaxSinglePass)
       return MCFFT_UNSUPPORTED_SIZE;
@@ -953,16 +971,67 @@ void link_group(mcfftPlan p, size_t first, int ndim, const int64_t* dims, int64_
   }
 }
 
-// Plan-time tuning of a 1D four-step group's split n = n1 * n2: besides
-// the default n1 = 2^floor(lg n / 2), the neighbouring splits (n1 / 2,
-// 2 n1) whose passes both run on the TMA-fed kernels are built and timed
-// on scratch buffers (each pass's median CUDA-event time, summed); the
-// fastest split wins when it is faster than the default by more than 3 %.
-// The choice is recorded as wisdom ("fourstep" records) and reported in
-// mcfftPlanInfo.fourstep_n1.  MCFFT_AUTOTUNE=0 or MCFFT_FOURSTEP_N1 keeps
-// the default (or the forced split).
+cudaError_t launch_one(mcfftPlan p, const Pass& ps, const void* src, void* dst, int dir,
+                       cudaStream_t st);
+int in_elem(const mcfftPlan p, const Pass& ps);
+int out_elem(const mcfftPlan p, const Pass& ps);
+
+// Median CUDA-event time (ms) of the passes [first, end) of the group being
+// built, launched as an exec would, on scratch buffers: `a` stands for the
+// user's input, `b` for the output and `c` for the plan's scratch (element
+// offsets taken relative to the group's own: in_off, out_off, soff0).
+float time_group(mcfftPlan p, size_t first, void* a, void* b, void* c, int64_t in_off,
+                 int64_t out_off, int64_t soff0) {
+  auto ptr = [&](int buf, int64_t off, int eb) -> char* {
+    if (buf == kUserIn) return (char*)a + (off - in_off) * eb;
+    if (buf == kUserOut) return (char*)b + (off - out_off) * eb;
+    return (char*)c + (off - soff0) * eb;
+  };
+  auto run = [&]() -> bool {
+    for (size_t i = first; i < p->passes.size(); ++i) {
+      const Pass& ps = p->passes[i];
+      if (launch_one(p, ps, ptr(ps.in_buf, ps.in_off, in_elem(p, ps)),
+                     ptr(ps.out_buf, ps.out_off, out_elem(p, ps)), 0, 0) != cudaSuccess)
+        return false;
+    }
+    return true;
+  };
+  cudaEvent_t e0, e1;
+  if (cudaEventCreate(&e0) != cudaSuccess) return -1.f;
+  if (cudaEventCreate(&e1) != cudaSuccess) {
+    cudaEventDestroy(e0);
+    return -1.f;
+  }
+  float t[5] = {0};
+  bool ok = run() && run();
+  for (int r = 0; r < 5 && ok; ++r)
+    ok = cudaEventRecord(e0, 0) == cudaSuccess && run() && cudaEventRecord(e1, 0) == cudaSuccess &&
+         cudaEventSynchronize(e1) == cudaSuccess && cudaEventElapsedTime(&t[r], e0, e1) == cudaSuccess;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (!ok) {
+    cudaGetLastError();
+    return -1.f;
+  }
+  std::sort(t, t + 5);
+  return t[2];
+}
+
+// Plan-time choice of a 1D group's decomposition past one pass.  The
+// candidates are the untuned default (default_lg1), the four-step splits
+// n = n1 * n2 with n1 = 2^floor(lg n / 2) and its neighbours n1 / 2 and
+// 2 n1, and, from n = 2^21 on, the three-pass plan n = n1 * n2 * n3.  Each is built and timed on scratch
+// buffers as an exec runs it (median CUDA-event time of the whole group);
+// the fastest wins when it beats the default by more than 3 %.  A split
+// whose factor exceeds the tile kernels' range runs a direct-load pass, and
+// the timing decides between it and three tile passes: the four-step pair
+// of 2^25 and 2^26 points has such a factor (8192), the three-pass plan
+// does not.  The choice is recorded as wisdom ("fourstep" records: lg n1,
+// or -1 for three passes) and reported in mcfftPlanInfo.fourstep_n1.
+// MCFFT_AUTOTUNE=0, MCFFT_FOURSTEP_N1 or MCFFT_THREE_PASS keep the default
+// (or the forced plan).
 int tune_fourstep(mcfftPlan p, int64_t n, int64_t batch, int64_t in_off, int64_t out_off) {
-  const int lg = ilog2(n), def = lg / 2;
+  const int lg = ilog2(n), def = default_lg1(p, n);
   if (n <= (p->split ? kMaxTilePass / 2 : kMaxTilePass) || n > kMaxSinglePass * kMaxSinglePass)
     return 0;
   if (std::getenv("MCFFT_FOURSTEP_N1") || std::getenv("MCFFT_THREE_PASS")) return 0;
@@ -976,7 +1045,9 @@ int tune_fourstep(mcfftPlan p, int64_t n, int64_t batch, int64_t in_off, int64_t
   // each candidate's passes are built, timed, then removed again
   const size_t first = p->passes.size();
   const size_t scratch0 = p->scratch_bytes;
+  const bool no_queue0 = p->no_queue;
   const size_t eb = p->split ? 8 : 4;
+  const int64_t soff0 = (int64_t)(scratch0 / eb);
   void *a = nullptr, *b = nullptr, *c = nullptr;
   const size_t bytes = (size_t)n * batch * eb;
   if (cudaMalloc(&a, bytes) != cudaSuccess || cudaMalloc(&b, bytes) != cudaSuccess ||
@@ -988,46 +1059,48 @@ int tune_fourstep(mcfftPlan p, int64_t n, int64_t batch, int64_t in_off, int64_t
     if (c) cudaFree(c);
     return 0;
   }
+  std::vector<int> cands = {def};
+  for (int lg1 : {lg / 2, lg / 2 - 1, lg / 2 + 1}) {
+    const int64_t n1 = int64_t(1) << lg1, n2 = n >> lg1;
+    if (lg1 != def && n1 >= 32 && n2 >= 32 && n1 <= kMaxSinglePass && n2 <= kMaxSinglePass)
+      cands.push_back(lg1);
+  }
+  if (lg >= 21 && def != kThreePass) cands.push_back(kThreePass);
   float best_t = -1.f, def_t = -1.f;
   int best = def;
-  for (int lg1 : {def, def - 1, def + 1}) {
-    const int64_t n1 = int64_t(1) << lg1, n2 = n >> lg1;
-    if (n1 < 32 || n2 < 32 || n1 > kMaxTilePass || n2 > kMaxTilePass) continue;
-    p->fs_lg1 = lg1;
+  for (int cand : cands) {
+    p->fs_lg1 = cand;
     int sl = 0;
     const mcfftResult r = build_group_passes(p, 1, &n, batch, in_off, out_off, &sl);
-    float t = 0.f;
-    bool ok = r == MCFFT_SUCCESS && p->passes.size() == first + 2;
-    for (size_t i = first; ok && i < p->passes.size(); ++i) {
-      const Pass& ps = p->passes[i];
-      if (!ps.tiled) {
-        ok = false;
-        break;
-      }
-      // pass 1 reads a and writes the scratch c; pass 2 reads c and writes b
-      const float ti = time_tile_pass(ps.tp, i == first ? a : c, i == first ? c : b, 0);
-      if (ti <= 0.f) ok = false;
-      t += ti;
-    }
+    const float t = r == MCFFT_SUCCESS ? time_group(p, first, a, b, c, in_off, out_off, soff0) : -1.f;
+    const size_t npasses = p->passes.size() - first;
+    int tiled = 0;
+    for (size_t i = first; i < p->passes.size(); ++i) tiled += p->passes[i].tiled ? 1 : 0;
     p->passes.resize(first);
     p->scratch_bytes = scratch0;
+    p->no_queue = no_queue0;
     p->fs_lg1 = 0;
-    if (!ok) continue;
+    if (t <= 0.f) continue;
     ++p->info.timed_passes;
-    if (std::getenv("MCFFT_DEBUG_PLAN"))
-      fprintf(stderr, "[mcfft] tune four-step n=%lld: n1=%lld %.4f ms\n", (long long)n,
-              (long long)n1, t);
-    if (lg1 == def) def_t = t;
+    if (std::getenv("MCFFT_DEBUG_PLAN")) {
+      if (cand == kThreePass)
+        fprintf(stderr, "[mcfft] tune 1D n=%lld: three passes (%zu launches) %.4f ms\n",
+                (long long)n, npasses, t);
+      else
+        fprintf(stderr, "[mcfft] tune 1D n=%lld: n1=%lld (%d of 2 passes tiled) %.4f ms\n",
+                (long long)n, (long long)(int64_t(1) << cand), tiled, t);
+    }
+    if (cand == def) def_t = t;
     if (best_t < 0.f || t < best_t) {
       best_t = t;
-      best = lg1;
+      best = cand;
     }
   }
   cudaFree(a);
   cudaFree(b);
   cudaFree(c);
   if (def_t > 0.f && best != def && best_t >= 0.97f * def_t) best = def;
-  if (def_t > 0.f) wisdom_put(key, best);
+  if (best_t > 0.f) wisdom_put(key, best);
   return best;
 }
 
@@ -1036,7 +1109,7 @@ mcfftResult build_group(mcfftPlan p, int ndim, const int64_t* dims, int64_t batc
   const size_t first = p->passes.size();
   p->fs_lg1 = ndim == 1 ? tune_fourstep(p, dims[0], batch, in_off, out_off) : 0;
   mcfftResult r = build_group_passes(p, ndim, dims, batch, in_off, out_off, scale_log2);
-  if (!r && ndim == 1 && first == 0 && p->passes.size() == 2)
+  if (!r && ndim == 1 && first == 0 && p->passes.size() >= 2)
     p->info.fourstep_n1 = p->passes[0].spec.L;
   p->fs_lg1 = 0;
   int64_t points = batch;
@@ -1467,39 +1540,45 @@ mcfftResult exec_graph(mcfftPlan p, const void* in, void* out, int dir, cudaStre
   return MCFFT_SUCCESS;
 }
 
+// One pass on the stream: `src` and `dst` are its input and output with
+// the pass's element offsets already applied.
+cudaError_t launch_one(mcfftPlan p, const Pass& ps, const void* src, void* dst, int dir,
+                       cudaStream_t st) {
+  if (ps.tiled) {
+    cudaError_t e = launch_tile_pass(ps.tp, src, dst, dir, st);
+    if (e == cudaSuccess && std::getenv("MCFFT_DEBUG_SYNC")) {
+      e = cudaStreamSynchronize(st);
+      fprintf(stderr, "[mcfft] tile pass L=%d R=%d C=%d grid=%d tiles=%lld: %s\n", ps.tp.k->L,
+              ps.tp.k->R, ps.tp.k->C, ps.tp.grid, (long long)ps.tp.args.ntiles,
+              cudaGetErrorString(e));
+    }
+    return e;
+  }
+  PassArgs a = ps.a;
+  a.in = src;
+  a.out = dst;
+  a.tw = ps.tw[dir];
+  a.tail_tw = ps.tail[dir];
+  a.post_lo = ps.plo[dir];
+  a.post_hi = ps.phi[dir];
+  a.bmat = p->bmat[dir];
+  a.bmat_lo = p->bmat_lo[dir];
+  a.inverse = dir;
+  return launch_pass(*ps.k, a, ps.grid, st);
+}
+
+// Element size (bytes) at the input / output end of a pass.
+int in_elem(const mcfftPlan p, const Pass& ps) { return p->split ? (ps.in_f16 ? 4 : 8) : 4; }
+int out_elem(const mcfftPlan p, const Pass& ps) { return p->split ? (ps.out_f16 ? 4 : 8) : 4; }
+
 mcfftResult exec_launches(mcfftPlan p, const void* in, void* out, int dir, cudaStream_t st) {
   if (p->q.on) return exec_queue(p, in, out, dir, st);
   for (auto& ps : p->passes) {
-    PassArgs a = ps.a;
     auto base = [&](int b) -> char* {
       return b == kUserIn ? (char*)const_cast<void*>(in) : b == kUserOut ? (char*)out : (char*)p->scratch;
     };
-    const int ib = p->split ? (ps.in_f16 ? 4 : 8) : 4;
-    const int ob = p->split ? (ps.out_f16 ? 4 : 8) : 4;
-    a.in = base(ps.in_buf) + ps.in_off * ib;
-    a.out = base(ps.out_buf) + ps.out_off * ob;
-    if (ps.tiled) {
-      cudaError_t e = launch_tile_pass(ps.tp, a.in, a.out, dir, st);
-      if (e == cudaSuccess && std::getenv("MCFFT_DEBUG_SYNC")) {
-        e = cudaStreamSynchronize(st);
-        fprintf(stderr, "[mcfft] tile pass L=%d R=%d C=%d grid=%d tiles=%lld: %s\n", ps.tp.k->L,
-                ps.tp.k->R, ps.tp.k->C, ps.tp.grid, (long long)ps.tp.args.ntiles,
-                cudaGetErrorString(e));
-      }
-      if (e != cudaSuccess) {
-        cudaGetLastError();
-        return MCFFT_CUDA_ERROR;
-      }
-      continue;
-    }
-    a.tw = ps.tw[dir];
-    a.tail_tw = ps.tail[dir];
-    a.post_lo = ps.plo[dir];
-    a.post_hi = ps.phi[dir];
-    a.bmat = p->bmat[dir];
-    a.bmat_lo = p->bmat_lo[dir];
-    a.inverse = dir;
-    cudaError_t e = launch_pass(*ps.k, a, ps.grid, st);
+    cudaError_t e = launch_one(p, ps, base(ps.in_buf) + ps.in_off * in_elem(p, ps),
+                               base(ps.out_buf) + ps.out_off * out_elem(p, ps), dir, st);
     if (e != cudaSuccess) {
       cudaGetLastError();
       return MCFFT_CUDA_ERROR;
@@ -1902,8 +1981,10 @@ mcfftResult mcfftWisdomImport(const char* path) {
     char* end = nullptr;
     const long tp = std::strtol(v.c_str(), &end, 10);
     // tile-shape records hold 8192 or 16384 points; four-step records lg n1
+    // (4..13) or -1 (three passes)
     const bool fs = l.find("\tfourstep ") != std::string::npos;
-    if (v.empty() || *end || (fs ? (tp < 4 || tp > 13) : (tp != 8192 && tp != 16384))) {
+    const bool fs_ok = (tp >= 4 && tp <= 13) || tp == kThreePass;
+    if (v.empty() || *end || (fs ? !fs_ok : (tp != 8192 && tp != 16384))) {
       ok = false;
       break;
     }

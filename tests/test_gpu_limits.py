@@ -1,8 +1,9 @@
 """The plan builder's size limits, at the limits.
 
 The largest transforms a plan accepts run against the FP64 oracle in both
-forms: 1D 2^26 (the four-step pair of passes of 8192 points each), 1D 2^27
-(three passes of 512 points: the reference's largest 1D size), 2D
+forms: 1D 2^25 and 2^26 (three passes of 256-512 points unless the plan-time
+tuner measures a four-step pair with a direct-load 8192-point pass faster),
+1D 2^27 (three passes of 512 points: the reference's largest 1D size), 2D
 8192 x 8192, and a 3D side of 8192 on each axis in turn.  The first sizes
 past the limits, and sizes that are not powers of two or are below 16, are
 refused with MCFFT_UNSUPPORTED_SIZE (an error, never a fallback).
@@ -27,7 +28,7 @@ from tests.gpu_util import compare, rand_complex, rounded, run  # noqa: E402
 PLAIN_TOL = 1e-3
 SPLIT_TOL = 2e-6
 
-BIG = [(1 << 26,), (1 << 27,), (8192, 8192)]
+BIG = [(1 << 25,), (1 << 26,), (1 << 27,), (8192, 8192)]
 SIDES_3D = [(8192, 16, 16), (16, 8192, 16), (16, 16, 8192)]
 
 _refs = {}

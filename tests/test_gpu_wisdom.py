@@ -64,3 +64,37 @@ def test_non_default_fourstep_splits(prec, n1, monkeypatch):
     ref = oracle.fft1d(rounded(x, f16)) * 2.0 ** sl
     rel, _ = compare(y, ref)
     assert rel < (1e-3 if f16 else 2e-6), rel
+
+
+def test_three_pass_choice_from_wisdom(tmp_path):
+    """From 2^21 points the tuner also times the three-pass plan; a record
+    that names it (-1) makes a later plan take three passes without timing
+    the decompositions, with results inside the plain form's tolerance."""
+    n, batch = 1 << 22, 2
+    x = rand_complex((batch, n), seed=41)
+    mc.wisdom_forget()
+    try:
+        with mc.Plan((n,), batch, mc.PREC_FP16) as p:
+            info = p.info()
+            # three four-step splits and the three-pass plan, then the
+            # chosen plan's tiled passes
+            assert info.timed_passes >= 4 + 2, info.timed_passes
+        path = str(tmp_path / "wisdom.txt")
+        mc.wisdom_export(path)
+        lines = open(path).read().splitlines()
+        fs = [ln for ln in lines if "\tfourstep n4194304 " in ln]
+        assert len(fs) == 1, lines
+        forced = [ln.rsplit("\t", 1)[0] + "\t-1" if ln in fs else ln for ln in lines]
+        (tmp_path / "forced.txt").write_text("\n".join(forced) + "\n")
+        mc.wisdom_forget()
+        mc.wisdom_import(str(tmp_path / "forced.txt"))
+        with mc.Plan((n,), batch, mc.PREC_FP16) as p:
+            info = p.info()
+            assert info.num_passes == 2 + batch  # three passes, the last per transform
+            assert info.fourstep_n1 == 1 << 7  # n = 2^7 * 2^7 * 2^8
+            y, sl = run(p, x, True)
+        ref = oracle.fft1d(rounded(x, True)) * 2.0 ** sl
+        rel, _ = compare(y, ref)
+        assert rel < 1e-3, rel
+    finally:
+        mc.wisdom_forget()
