@@ -900,6 +900,11 @@ __global__ void __maxnreg__(NCW <= 8 ? 80 : 96) fft_tile_f16(const __grid_consta
   sm100::tc_fence_before();
   __syncthreads();
   sm100::tc_fence_after();
+  // The setup above reads only this launch's constant tables, so under a
+  // programmatic dependent launch it overlaps the previous pass's last
+  // tiles; the buffers the passes share are touched only from here on.
+  sm100::grid_dep_wait();
+  sm100::grid_dep_launch();
   const uint32_t tmem_base = *tmem_slot;
   const TileCtx x{sS0, sS1, sA, sB, sTail, sTws, bS0, bS1, bA, tmem_base, mmab, abort_flag};
 

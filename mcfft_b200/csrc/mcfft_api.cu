@@ -972,7 +972,7 @@ void link_group(mcfftPlan p, size_t first, int ndim, const int64_t* dims, int64_
 }
 
 cudaError_t launch_one(mcfftPlan p, const Pass& ps, const void* src, void* dst, int dir,
-                       cudaStream_t st);
+                       cudaStream_t st, bool follows);
 int in_elem(const mcfftPlan p, const Pass& ps);
 int out_elem(const mcfftPlan p, const Pass& ps);
 
@@ -991,7 +991,7 @@ float time_group(mcfftPlan p, size_t first, void* a, void* b, void* c, int64_t i
     for (size_t i = first; i < p->passes.size(); ++i) {
       const Pass& ps = p->passes[i];
       if (launch_one(p, ps, ptr(ps.in_buf, ps.in_off, in_elem(p, ps)),
-                     ptr(ps.out_buf, ps.out_off, out_elem(p, ps)), 0, 0) != cudaSuccess)
+                     ptr(ps.out_buf, ps.out_off, out_elem(p, ps)), 0, 0, i > first) != cudaSuccess)
         return false;
     }
     return true;
@@ -1540,12 +1540,24 @@ mcfftResult exec_graph(mcfftPlan p, const void* in, void* out, int dir, cudaStre
   return MCFFT_SUCCESS;
 }
 
+// Programmatic dependent launch of a plan's later tile passes (their setup
+// overlaps the previous pass's last tiles); MCFFT_PDL=0 launches every pass
+// in plain stream order.
+bool pdl_on() {
+  static const bool on = [] {
+    const char* e = std::getenv("MCFFT_PDL");
+    return !e || std::atoi(e) != 0;
+  }();
+  return on;
+}
+
 // One pass on the stream: `src` and `dst` are its input and output with
-// the pass's element offsets already applied.
+// the pass's element offsets already applied.  `follows`: a pass of the
+// same exec ran just before on the stream.
 cudaError_t launch_one(mcfftPlan p, const Pass& ps, const void* src, void* dst, int dir,
-                       cudaStream_t st) {
+                       cudaStream_t st, bool follows) {
   if (ps.tiled) {
-    cudaError_t e = launch_tile_pass(ps.tp, src, dst, dir, st);
+    cudaError_t e = launch_tile_pass(ps.tp, src, dst, dir, st, follows && pdl_on());
     if (e == cudaSuccess && std::getenv("MCFFT_DEBUG_SYNC")) {
       e = cudaStreamSynchronize(st);
       fprintf(stderr, "[mcfft] tile pass L=%d R=%d C=%d grid=%d tiles=%lld: %s\n", ps.tp.k->L,
@@ -1573,12 +1585,13 @@ int out_elem(const mcfftPlan p, const Pass& ps) { return p->split ? (ps.out_f16 
 
 mcfftResult exec_launches(mcfftPlan p, const void* in, void* out, int dir, cudaStream_t st) {
   if (p->q.on) return exec_queue(p, in, out, dir, st);
-  for (auto& ps : p->passes) {
+  for (size_t i = 0; i < p->passes.size(); ++i) {
+    const Pass& ps = p->passes[i];
     auto base = [&](int b) -> char* {
       return b == kUserIn ? (char*)const_cast<void*>(in) : b == kUserOut ? (char*)out : (char*)p->scratch;
     };
     cudaError_t e = launch_one(p, ps, base(ps.in_buf) + ps.in_off * in_elem(p, ps),
-                               base(ps.out_buf) + ps.out_off * out_elem(p, ps), dir, st);
+                               base(ps.out_buf) + ps.out_off * out_elem(p, ps), dir, st, i > 0);
     if (e != cudaSuccess) {
       cudaGetLastError();
       return MCFFT_CUDA_ERROR;

@@ -78,6 +78,17 @@ __device__ __forceinline__ void tc_fence_after() {
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 }
 
+// ------------------------------------------------ programmatic dependent launch
+// A grid launched with programmatic stream serialization may start while
+// the previous grid on the stream is still running.  grid_dep_wait blocks
+// until that grid has completed and its memory writes are visible (at once
+// for a grid launched without the attribute); grid_dep_launch lets the next
+// such grid start once every CTA of this one has issued it or exited.
+__device__ __forceinline__ void grid_dep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void grid_dep_launch() {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 // ------------------------------------------------------------------- TMEM
 // Warp-collective.  Writes the allocated TMEM base address to *dst (smem).
 __device__ __forceinline__ void tmem_alloc(uint32_t* dst, uint32_t ncols) {

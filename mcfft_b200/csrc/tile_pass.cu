@@ -159,7 +159,7 @@ bool tile_check_encode(const layout::Staging& s, const void* probe) {
 }
 
 cudaError_t launch_tile_pass(const TilePass& tp, const void* in, void* out, int dir,
-                             cudaStream_t st) {
+                             cudaStream_t st, bool pdl) {
   TileArgs a = tp.args;
   if (!encode(&a.tmap_in, tp.lay.in, in) || !encode(&a.tmap_out, tp.lay.out, out))
     return cudaErrorInvalidValue;
@@ -187,8 +187,17 @@ cudaError_t launch_tile_pass(const TilePass& tp, const void* in, void* out, int 
     }
   }
   void* args[] = {&a};
-  return cudaLaunchKernel(tp.k->fn, dim3(tp.grid), dim3(tp.k->nthreads), args,
-                          (size_t)tp.k->smem_bytes, st);
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(tp.grid);
+  cfg.blockDim = dim3(tp.k->nthreads);
+  cfg.dynamicSmemBytes = (size_t)tp.k->smem_bytes;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = pdl ? 1 : 0;
+  return cudaLaunchKernelExC(&cfg, tp.k->fn, args);
 }
 
 void fill_tile_args(TilePass* tp) {

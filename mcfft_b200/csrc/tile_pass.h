@@ -48,8 +48,11 @@ bool tile_layout(layout::PassLayout* out, int L, int R, int C, layout::Kind ik, 
 bool tile_check_encode(const layout::Staging& s, const void* probe);
 bool tile_encode(CUtensorMap* map, const layout::Staging& s, const void* base);
 void fill_tile_args(TilePass* tp);
+// pdl: launch with programmatic stream serialization (the kernel's setup
+// may overlap the previous kernel on the stream; it waits for that kernel's
+// completion before touching `in` or `out`).
 cudaError_t launch_tile_pass(const TilePass& tp, const void* in, void* out, int dir,
-                             cudaStream_t st);
+                             cudaStream_t st, bool pdl = false);
 
 // DFT-16 embedding times `scale` (a power of two) in the 64-byte-swizzled
 // K-major layout the tile kernel reads (row j = output component, K = 16
