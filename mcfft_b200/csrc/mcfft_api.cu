@@ -738,7 +738,14 @@ mcfftResult add_pass(mcfftPlan p, const PassSpec& s) {
 }
 
 constexpr int64_t kMaxSinglePass = 8192;
-constexpr int64_t kMaxTilePass = 4096;  // 1D lengths above run as four-step (split: 2048)
+constexpr int64_t kMaxTilePass = 4096;  // 1D lengths above run as four-step
+
+// The longest 1D transform one pass takes: 4096 points, in the split form
+// only outside the batch queue (whose split tiles hold at most 2048 points
+// per column; a plan bound for it runs 4096 as a four-step pair).
+int64_t max_one_pass(const mcfftPlan p) {
+  return p->split && p->queue_planned ? kMaxTilePass / 2 : kMaxTilePass;
+}
 
 constexpr int64_t kMaxLength1d = int64_t(1) << 27;
 
@@ -818,8 +825,7 @@ mcfftResult build_group_passes(mcfftPlan p, int ndim, const int64_t* dims, int64
   *scale_log2 = split ? 0 : -ilog2(total);
   if (ndim == 1) {
     const int64_t n = dims[0];
-    // the split tile kernel's 8K-point tiles hold at most L = 2048
-    if (n <= (split ? kMaxTilePass / 2 : kMaxTilePass)) {
+    if (n <= max_one_pass(p)) {
       PassSpec s{n, false, false, 1, n, 0, 1, n, 0, batch, 1, kUserIn, kUserOut, 0,
                  in_f16, split ? 0 : 1, in_off, out_off};
       return add_pass(p, s);
@@ -1032,8 +1038,7 @@ float time_group(mcfftPlan p, size_t first, void* a, void* b, void* c, int64_t i
 // (or the forced plan).
 int tune_fourstep(mcfftPlan p, int64_t n, int64_t batch, int64_t in_off, int64_t out_off) {
   const int lg = ilog2(n), def = default_lg1(p, n);
-  if (n <= (p->split ? kMaxTilePass / 2 : kMaxTilePass) || n > kMaxSinglePass * kMaxSinglePass)
-    return 0;
+  if (n <= max_one_pass(p) || n > kMaxSinglePass * kMaxSinglePass) return 0;
   if (std::getenv("MCFFT_FOURSTEP_N1") || std::getenv("MCFFT_THREE_PASS")) return 0;
   if (const char* e = std::getenv("MCFFT_AUTOTUNE"))
     if (std::atoi(e) == 0) return 0;

@@ -1,6 +1,9 @@
 // tile_split.cu -- registry of the split-form tile kernel variants
 // (fft_tile_split.cuh): 8K-point tiles, 16 consumer warps, one CTA per SM,
 // FP16 or FP32 input staging, with and without the four-step twiddle.
+// L = 4096 holds two columns per tile, which only row staging takes (the
+// layout engine refuses it for column passes); the batch kernel has no
+// such variant.
 #include <vector>
 
 #include "fft_tile_split.cuh"
@@ -25,7 +28,7 @@ TileKernel make_split() {
   make_split<32, 2, PT, IN16>(), make_split<64, 4, PT, IN16>(),                         \
       make_split<128, 8, PT, IN16>(), make_split<256, 1, PT, IN16>(),                   \
       make_split<512, 2, PT, IN16>(), make_split<1024, 4, PT, IN16>(),                  \
-      make_split<2048, 8, PT, IN16>()
+      make_split<2048, 8, PT, IN16>(), make_split<4096, 1, PT, IN16>()
 
 }  // namespace
 

@@ -93,6 +93,24 @@ def test_split_layouts(checker, L, R, C, ik, ok, ie):
         assert pro == pytest.approx(0.0, abs=1e-9)
 
 
+@pytest.mark.parametrize("ie", [8, 4])
+def test_split_two_column_row_layout(checker, ie):
+    """Split form, L = 4096 in 8K-point tiles (two columns): row-in /
+    row-out only, FP32 or FP16 input staging, FP32 output; tables
+    consistent and the epilogue conflict-free.  Column staging is refused."""
+    r = subprocess.run([checker, "4096", "1", "2", "row", "row", str(ie), "8"],
+                       capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stdout + r.stderr
+    out = dict(line.split(None, 1) for line in r.stdout.splitlines())
+    assert out["tables_consistent"] == "1"
+    assert out["epilogue_consistent"] == "1"
+    assert float(out["epilogue_excess"]) == pytest.approx(0.0, abs=1e-9)
+    for ik, ok in (("col", "col"), ("row", "col")):
+        r = subprocess.run([checker, "4096", "1", "2", ik, ok, str(ie), "8"], capture_output=True,
+                           text=True, timeout=120)
+        assert r.returncode == 1 and r.stdout.startswith("error"), r.stdout
+
+
 PLAIN_8K_SHAPES = [  # L, R, C (8K-point tiles of the plain form, and L = 32 at 16K)
     (32, 2, 256), (64, 4, 128), (128, 8, 64), (256, 1, 32), (512, 2, 16), (1024, 4, 8),
     (2048, 8, 4), (32, 2, 512),
