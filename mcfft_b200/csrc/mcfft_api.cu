@@ -1392,6 +1392,17 @@ mcfftResult build_queue(mcfftPlan p) {
   if (order.empty()) return MCFFT_SUCCESS;  // no consistent order: pass by pass
   std::vector<QItem> items(order.size());
   for (size_t i = 0; i < order.size(); ++i) items[i] = {order[i].pass, order[i].tile};
+  if (std::getenv("MCFFT_DEBUG_PLAN")) {
+    // runs: stretches of one CTA's items (i, i + G, ..) on one pass; each
+    // run reloads the pass's tables
+    int64_t runs = 0;
+    for (int64_t b = 0; b < G; ++b)
+      for (int64_t i = b; i < (int64_t)items.size(); i += G)
+        runs += (i < G || items[i].pass != items[i - G].pass) ? 1 : 0;
+    fprintf(stderr, "[mcfft] queue: %zu passes, %zu items on %lld CTAs, %lld runs (%.2f items per run)\n",
+            np, items.size(), (long long)G, (long long)runs,
+            runs ? (double)items.size() / (double)runs : 0.0);
+  }
   mcfftResult r = plan_alloc(p, &q.items, items.size() * sizeof(QItem));
   if (!r) r = plan_alloc(p, &q.counters, (size_t)std::max<int64_t>(nc, 1) * sizeof(int));
   if (r) return r;

@@ -40,10 +40,14 @@ TileKernel make_f16() {
       make_f16<512, 2, PT, TP, NCW>(), make_f16<1024, 4, PT, TP, NCW>(),                  \
       make_f16<2048, 8, PT, TP, NCW>(), make_f16<4096, 1, PT, TP, NCW>()
 
+// L = 16 (one radix-16 stage, 1024 or 512 columns per tile): column passes
+// only (the layout engine has no row staging for it), never with the
+// four-step twiddle; the sides of 16 of 2D and 3D transforms.
 const std::vector<TileKernel>& registry() {
   static const std::vector<TileKernel> v = {
       MCFFT_TILE_VARIANTS(false, 16384, 16), MCFFT_TILE_VARIANTS(true, 16384, 16),
-      MCFFT_TILE_VARIANTS(false, 8192, 16), MCFFT_TILE_VARIANTS(true, 8192, 16)};
+      MCFFT_TILE_VARIANTS(false, 8192, 16), MCFFT_TILE_VARIANTS(true, 8192, 16),
+      make_f16<16, 1, false, 16384, 16>(), make_f16<16, 1, false, 8192, 16>()};
   return v;
 }
 

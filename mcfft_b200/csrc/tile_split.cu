@@ -3,7 +3,7 @@
 // FP16 or FP32 input staging, with and without the four-step twiddle.
 // L = 4096 holds two columns per tile, which only row staging takes (the
 // layout engine refuses it for column passes); the batch kernel has no
-// such variant.
+// such variant.  L = 16 (512 columns per tile) serves column passes only.
 #include <vector>
 
 #include "fft_tile_split.cuh"
@@ -35,7 +35,8 @@ TileKernel make_split() {
 const std::vector<TileKernel>& split_registry() {
   static const std::vector<TileKernel> v = {
       MCFFT_SPLIT_VARIANTS(false, false), MCFFT_SPLIT_VARIANTS(true, false),
-      MCFFT_SPLIT_VARIANTS(false, true), MCFFT_SPLIT_VARIANTS(true, true)};
+      MCFFT_SPLIT_VARIANTS(false, true), MCFFT_SPLIT_VARIANTS(true, true),
+      make_split<16, 1, false, false>(), make_split<16, 1, false, true>()};
   return v;
 }
 

@@ -62,7 +62,7 @@ def test_split_1d_f16_input(n, batch):
 @pytest.mark.parametrize("prec", [mc.PREC_FP16, mc.PREC_SPLIT])
 @pytest.mark.parametrize("nx,ny,batch", [(16, 16, 4), (128, 256, 2), (256, 128, 2), (512, 512, 1),
                                          (1024, 1024, 1), (64, 2048, 1), (2048, 256, 1),
-                                         (32, 4096, 2)])
+                                         (32, 4096, 2), (16, 1024, 3)])
 def test_2d(prec, nx, ny, batch):
     f16 = prec == mc.PREC_FP16
     x = rand_complex((batch, nx, ny), seed=nx + ny)
@@ -83,7 +83,8 @@ def test_2d_wide_range_split():
 
 
 @pytest.mark.parametrize("prec", [mc.PREC_FP16, mc.PREC_SPLIT])
-@pytest.mark.parametrize("dims", [(16, 16, 16), (32, 64, 128), (64, 64, 64), (256, 256, 32)])
+@pytest.mark.parametrize("dims", [(16, 16, 16), (32, 64, 128), (64, 64, 64), (256, 256, 32),
+                                  (64, 16, 128)])
 def test_3d(prec, dims):
     f16 = prec == mc.PREC_FP16
     x = rand_complex((1,) + dims, seed=3)

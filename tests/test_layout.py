@@ -111,6 +111,25 @@ def test_split_two_column_row_layout(checker, ie):
         assert r.returncode == 1 and r.stdout.startswith("error"), r.stdout
 
 
+@pytest.mark.parametrize("C,ie,oe", [(1024, 4, 4), (512, 4, 4), (512, 8, 8), (512, 4, 8)])
+def test_sixteen_point_column_layout(checker, C, ie, oe):
+    """L = 16 (one radix-16 stage): column staging in the plain form (16K- and
+    8K-point tiles) and the split form (FP32 or FP16 input, FP32 output);
+    tables consistent, epilogue conflict-free.  Row staging is refused (the
+    sides of 16 along the contiguous axis keep the direct-load kernel)."""
+    r = subprocess.run([checker, "16", "1", str(C), "col", "col", str(ie), str(oe)],
+                       capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stdout + r.stderr
+    out = dict(line.split(None, 1) for line in r.stdout.splitlines())
+    assert out["tables_consistent"] == "1"
+    assert out["epilogue_consistent"] == "1"
+    assert float(out["epilogue_excess"]) == pytest.approx(0.0, abs=1e-9)
+    assert float(out["prologue_excess"]) <= 1.0 + 1e-9
+    r = subprocess.run([checker, "16", "1", str(C), "row", "row", str(ie), str(oe)],
+                       capture_output=True, text=True, timeout=120)
+    assert r.returncode == 1 and r.stdout.startswith("error"), r.stdout
+
+
 PLAIN_8K_SHAPES = [  # L, R, C (8K-point tiles of the plain form, and L = 32 at 16K)
     (32, 2, 256), (64, 4, 128), (128, 8, 64), (256, 1, 32), (512, 2, 16), (1024, 4, 8),
     (2048, 8, 4), (32, 2, 512),
