@@ -227,15 +227,17 @@ __device__ __forceinline__ int64_t run_items(const QArgs& a, uint32_t pi, const 
   static_assert(RESIDENT || !TL::T::TW_SMEM || TL::T::TW_ROWS * 128 <= QueueSmem::TWS_BYTES,
                 "stage rows");
   const QPass& P = a.pass[pi];
+  // The layout entries' loads are issued first, so that they are in flight
+  // while the tables are copied (one L2 round trip per run instead of two).
+  uint2 ient[TL::NIT_P];
+  uint32_t eent[TL::NST][TL::NIT_E];
+  TL::entries(P, ctid, ient, eent);
   if constexpr (!RESIDENT) {
     // every consumer is past the previous tile's last barrier, so nobody
     // still reads the old tables
     TL::tables(P, smem + QueueSmem::OFF_TAIL, smem + QueueSmem::OFF_TWS, ctid);
     tile::named_bar(1, TL::NCT);
   }
-  uint2 ient[TL::NIT_P];
-  uint32_t eent[TL::NST][TL::NIT_E];
-  TL::entries(P, ctid, ient, eent);
   volatile int* abort_flag;
   if constexpr (SPLIT) abort_flag = x.t.abort_flag;
   else abort_flag = x.abort_flag;
