@@ -31,7 +31,7 @@
  *                     (scale_log2 = 0), like FFTW_FORWARD/FFTW_BACKWARD.
  *
  * Sizes: every dimension a power of two >= 16; 1D lengths up to 2^27 (one
- * pass up to 4096; past that a four-step pair of passes,
+ * pass up to 8192, split form 4096; past that a four-step pair of passes,
  * or three passes from 2^24 points (split form 2^23) and for 2^27, the
  * decomposition tuned at plan time); 2D/3D sides up to 8192 (one pass per
  * axis).

@@ -347,7 +347,10 @@ struct TileF16 {
   // 16 KB (all L but 4096 with R = 1, whose rows are read through L1).
   static constexpr int TW_ROWS = stage_tw_rows<L, R>();
   static constexpr bool TW_SMEM = TW_ROWS <= 128;
-  static constexpr int TAIL_BYTES = R > 1 ? L * 8 : 0;
+  // L = 8192 (R = 2, two columns per 16K-point tile): the radix-2 table
+  // (64 KB) does not fit beside the tile; its twiddles are computed.
+  static constexpr bool TAIL_CALC = R == 2 && L >= 8192;
+  static constexpr int TAIL_BYTES = R > 1 && !TAIL_CALC ? L * 8 : 0;
   static constexpr int TWS_BYTES = TW_SMEM ? TW_ROWS * 128 : 0;
   static constexpr int OFF_S0 = 0;
   static constexpr int OFF_S1 = STAGE_BYTES;
@@ -415,6 +418,23 @@ __device__ __forceinline__ __half2 h2muli(__half2 z, __half2 negpos) {
 // z * w with w given as (wr, wr) and (-wi, wi)
 __device__ __forceinline__ __half2 h2cmul(__half2 z, __half2 wrr, __half2 wni) {
   return __hfma2(h2swap(z), wni, __hmul2(z, wrr));
+}
+
+// The radix-2 prologue twiddle W_L^v / 2 (v < L / 2; sgn -1 forward, +1
+// inverse) as the packed pair {(wr, wr), (-wi, wi)} that h2cmul takes, for
+// the lengths whose table is not kept in shared memory: the angle
+// pi * v * (2 / L) is exact in FP32 before the product with pi and lies in
+// [0, pi), where the hardware sine and cosine are accurate to ~1e-6
+// absolute, far below the FP16 rounding of the pair.
+template <int L>
+__device__ __forceinline__ uint2 tail_tw_calc(uint32_t v, float sgn) {
+  float sn, cs;
+  __sincosf((float)v * (2.f / (float)L) * 3.14159265358979f, &sn, &cs);
+  const float wr = 0.5f * cs, wi = 0.5f * sgn * sn;
+  const __half2 wrr = __float2half2_rn(wr);
+  const __half2 wni = __floats2half2_rn(-wi, wi);
+  return make_uint2(*reinterpret_cast<const uint32_t*>(&wrr),
+                    *reinterpret_cast<const uint32_t*>(&wni));
 }
 
 template <int R>
@@ -551,7 +571,7 @@ struct F16Tile {
   // threads only.
   template <class A>
   static __device__ __forceinline__ void tables(const A& a, uint8_t* tail, uint8_t* tws, int ctid) {
-    if constexpr (R > 1) {
+    if constexpr (R > 1 && !T::TAIL_CALC) {
       for (int i = ctid; i < L; i += NCT) {
         const float2 w = __ldg(a.tail_tw + i);
         const __half2 wrr = __float2half2_rn(w.x);
@@ -635,7 +655,18 @@ struct F16Tile {
         }
       };
       constexpr int HP = NIT_P / 2;
-      if (NIT_P % 2 == 0 && S::ITEMS % NCT == 0 && a.tail_pm == kTailNaturalPaired) {
+      if constexpr (T::TAIL_CALC) {
+        // row items only (two-column tiles take row staging): sub-vector jj
+        // of item j has tail row v = trow + jj
+#pragma unroll
+        for (int j = 0; j < NIT_P; ++j) {
+          if (S::ITEMS % NCT != 0 && ctid + j * NCT >= S::ITEMS) break;
+          const uint32_t trow = ient[j].y & 0x7FFFFFFFu;
+#pragma unroll
+          for (int jj = 0; jj < 4; ++jj)
+            subvec(j, jj, tail_tw_calc<L>(trow + jj, tsgn), [&](int) { return make_uint4(0u, 0u, 0u, 0u); });
+        }
+      } else if (NIT_P % 2 == 0 && S::ITEMS % NCT == 0 && a.tail_pm == kTailNaturalPaired) {
         // Row items whose pairs (j, j + NIT_P / 2) read the same twiddle
         // rows (the layout guarantees it): each row is loaded once.
 #pragma unroll

@@ -7,7 +7,8 @@
 // length-L transform (L = 16^a * R) along one axis, and picks a tile shape
 // for each pass from the instantiated kernel variants.
 //
-//   1D, n <= 4096        one row pass (split form: n <= 2048)
+//   1D, n <= 8192        one row pass (split form: n <= 4096; a plan bound
+//                        for the batch kernel: 4096, split 2048)
 //   1D, larger n         four-step: n = n1 * n2; pass 1 = n1-point column
 //                        transforms (stride n2) with the W_n^(k1 n2)
 //                        twiddle fused into their epilogue, into a scratch
@@ -18,10 +19,12 @@
 //
 // All tables (stage twiddles, tail twiddles, four-step twiddles, the DFT-16
 // embedding) are generated in FP64 on the GPU at plan time for both
-// directions.  When every pass of a plan runs on the plain 16K-point tile
-// kernel, exec is one launch of the persistent batch kernel (fft_queue.cuh)
-// over a queue of (pass, tile) items built here; otherwise one launch per
-// pass.
+// directions; the plain form's four-step twiddles and the radix-2 twiddles
+// of 8192-point passes are instead computed in the kernel from their exact
+// angle.  A plan of several transform groups (mcfftPlanCreateBatch) whose
+// passes all run on tile kernels the batch kernel holds executes as one
+// launch of the persistent batch kernel (fft_queue.cuh) over a queue of
+// (pass, tile) items built here; otherwise one launch per pass.
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
@@ -738,13 +741,16 @@ mcfftResult add_pass(mcfftPlan p, const PassSpec& s) {
 }
 
 constexpr int64_t kMaxSinglePass = 8192;
-constexpr int64_t kMaxTilePass = 4096;  // 1D lengths above run as four-step
+constexpr int64_t kMaxTilePass = 4096;  // longest column of the four-column tiles
 
-// The longest 1D transform one pass takes: 4096 points, in the split form
-// only outside the batch queue (whose split tiles hold at most 2048 points
-// per column; a plan bound for it runs 4096 as a four-step pair).
+// The longest 1D transform one pass takes: 8192 points in the plain form
+// (two per 16K-point tile) and 4096 in the split form (two per 8K-point
+// tile), outside the batch queue; a plan bound for it takes only the tile
+// shapes the batch kernel holds (4096, split 2048) and runs longer lengths
+// as four-step pairs.
 int64_t max_one_pass(const mcfftPlan p) {
-  return p->split && p->queue_planned ? kMaxTilePass / 2 : kMaxTilePass;
+  if (p->queue_planned) return p->split ? kMaxTilePass / 2 : kMaxTilePass;
+  return p->split ? kMaxTilePass : 2 * kMaxTilePass;
 }
 
 constexpr int64_t kMaxLength1d = int64_t(1) << 27;

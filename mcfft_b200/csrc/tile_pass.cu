@@ -42,12 +42,15 @@ TileKernel make_f16() {
 
 // L = 16 (one radix-16 stage, 1024 or 512 columns per tile): column passes
 // only (the layout engine has no row staging for it), never with the
-// four-step twiddle; the sides of 16 of 2D and 3D transforms.
+// four-step twiddle; the sides of 16 of 2D and 3D transforms.  L = 8192
+// (two columns per 16K-point tile, radix-2 twiddles computed): row-in /
+// row-out passes only (1D 8192 in one pass, rows of 8192).
 const std::vector<TileKernel>& registry() {
   static const std::vector<TileKernel> v = {
       MCFFT_TILE_VARIANTS(false, 16384, 16), MCFFT_TILE_VARIANTS(true, 16384, 16),
       MCFFT_TILE_VARIANTS(false, 8192, 16), MCFFT_TILE_VARIANTS(true, 8192, 16),
-      make_f16<16, 1, false, 16384, 16>(), make_f16<16, 1, false, 8192, 16>()};
+      make_f16<16, 1, false, 16384, 16>(), make_f16<16, 1, false, 8192, 16>(),
+      make_f16<8192, 2, false, 16384, 16>()};
   return v;
 }
 

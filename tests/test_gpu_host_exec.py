@@ -55,6 +55,10 @@ def exec_host(plan, hin, hout, direction=mc.FORWARD):
 def test_plain_chunked_matches_oracle_and_device_exec(monkeypatch, pinned):
     n, batch = 1 << 16, 32
     monkeypatch.setenv("MCFFT_HOST_CHUNK_BYTES", str(1 << 20))  # chunks of up to 4 transforms
+    # The chunk plans (1, 2, 4 transforms) are tuned apart from the full
+    # plan and may take another four-step split, whose FP16 roundings differ;
+    # untuned, every plan takes the same split and the outputs must agree.
+    monkeypatch.setenv("MCFFT_AUTOTUNE", "0")
     x = rand_complex((batch, n), seed=21)
     with mc.Plan((n,), batch, mc.PREC_FP16) as p:
         hin = host_in(x, True, pinned)

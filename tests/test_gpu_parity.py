@@ -24,7 +24,7 @@ PLAIN_TOL = 1e-3
 SPLIT_TOL = 2e-6
 
 SIZES_1D = [(16, 256), (32, 128), (64, 256), (128, 128), (256, 64), (512, 32), (1024, 16),
-            (2048, 8), (4096, 256), (8192, 4), (16384, 2), (32768, 2), (65536, 1),
+            (2048, 8), (4096, 256), (8192, 4), (8192, 33), (16384, 2), (32768, 2), (65536, 1),
             (1 << 20, 2), (1 << 22, 1)]
 
 

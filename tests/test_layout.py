@@ -136,15 +136,21 @@ PLAIN_8K_SHAPES = [  # L, R, C (8K-point tiles of the plain form, and L = 32 at 
 ]
 
 
-def test_two_column_row_layout(checker):
-    """L = 4096 in 8K-point tiles: two columns per tile, allowed for row-in /
-    row-out passes only (column staging needs four columns across its
-    16-byte TMA box)."""
-    out = run(checker, 4096, 1, 2, "row", "row")
+@pytest.mark.parametrize("L,R", [(4096, 1), (8192, 2)])
+def test_two_column_row_layout(checker, L, R):
+    """L = 4096 in 8K-point tiles and L = 8192 in 16K-point tiles: two
+    columns per tile, allowed for row-in / row-out passes only (column
+    staging needs four columns across its 16-byte TMA box); the epilogue
+    conflict-free."""
+    out = run(checker, L, R, 2, "row", "row")
     assert out["tables_consistent"] == "1"
     assert out["epilogue_consistent"] == "1"
+    assert float(out["epilogue_excess"]) == pytest.approx(0.0, abs=1e-9)
+    if R > 1:
+        # natural tail-twiddle rows: the kernel computes W^v / R for row v
+        assert int(out["tail_pm"]) == -1
     for ik, ok in (("col", "col"), ("row", "col")):
-        r = subprocess.run([checker, "4096", "1", "2", ik, ok], capture_output=True, text=True,
+        r = subprocess.run([checker, str(L), str(R), "2", ik, ok], capture_output=True, text=True,
                            timeout=120)
         assert r.returncode == 1 and r.stdout.startswith("error"), r.stdout
 
