@@ -755,19 +755,26 @@ int64_t max_one_pass(const mcfftPlan p) {
 
 constexpr int64_t kMaxLength1d = int64_t(1) << 27;
 
-// The three-pass decomposition as a choice of the four-step tuner (in
+// The three-pass decomposition, and the single pass of two columns per tile
+// (plain 8192, split 4096 points), as choices of the four-step tuner (in
 // mcfftPlan_st::fs_lg1 and in "fourstep" wisdom records).
 constexpr int kThreePass = -1;
+constexpr int kOnePass = -2;
 
-// The untuned decomposition of a 1D length past one pass: the four-step
-// split n1 = 2^floor(lg n / 2), or three passes from 2^24 points (plain
-// form) and 2^23 (split form).  Measured on a B200, 2^26 points in all per
+// The longest 1D transform of the four-column tiles (one pass, no choice).
+int64_t max_four_column(const mcfftPlan p) { return p->split ? kMaxTilePass / 2 : kMaxTilePass; }
+
+// The untuned decomposition of a 1D length past the four-column tiles: one
+// pass of two columns per tile where the form has it (plain 8192, split
+// 4096, outside the batch queue), the four-step split n1 = 2^floor(lg n /
+// 2), or three passes from 2^24 points (plain form) and 2^23 (split form).  Measured on a B200, 2^26 points in all per
 // exec: the split form's tile kernels hold at most 2048 points per column,
 // so its four-step pairs past 2^22 run a direct-load pass (2^23: 1.44 ms
 // against 0.80 ms in three passes); the plain form's pair of 4096-point
 // passes at 2^24 takes 0.65 ms against 0.41 ms in three, and past 2^24 its
 // pairs run a direct-load pass (2^26: 2.68 ms against 0.42 ms).
 int default_lg1(const mcfftPlan p, int64_t n) {
+  if (n <= max_one_pass(p)) return kOnePass;
   if (n >= (p->split ? (int64_t(1) << 23) : (int64_t(1) << 24))) return kThreePass;
   return ilog2(n) / 2;
 }
@@ -831,11 +838,9 @@ mcfftResult build_group_passes(mcfftPlan p, int ndim, const int64_t* dims, int64
   *scale_log2 = split ? 0 : -ilog2(total);
   if (ndim == 1) {
     const int64_t n = dims[0];
-    if (n <= max_one_pass(p)) {
-      PassSpec s{n, false, false, 1, n, 0, 1, n, 0, batch, 1, kUserIn, kUserOut, 0,
+    PassSpec one{n, false, false, 1, n, 0, 1, n, 0, batch, 1, kUserIn, kUserOut, 0,
                  in_f16, split ? 0 : 1, in_off, out_off};
-      return add_pass(p, s);
-    }
+    if (n <= max_four_column(p)) return add_pass(p, one);
     // MCFFT_THREE_PASS=1 takes the three-pass plan for every length past one
     // pass (a test switch: the same code path at sizes that test quickly)
     // MCFFT_FOURSTEP_N1 forces a four-step split
@@ -843,6 +848,8 @@ mcfftResult build_group_passes(mcfftPlan p, int ndim, const int64_t* dims, int64
     int lg1 = default_lg1(p, n);
     if (const char* e = std::getenv("MCFFT_FOURSTEP_N1")) lg1 = ilog2(std::atoll(e));
     if (p->fs_lg1 != 0) lg1 = p->fs_lg1;  // the plan-time tuner's choice or candidate
+    if (lg1 == kOnePass && n <= max_one_pass(p)) return add_pass(p, one);
+    if (lg1 == kOnePass) lg1 = ilog2(n) / 2;
     if (n > kMaxSinglePass * kMaxSinglePass || (three && std::atoi(three) != 0 && n >= 4096 * 16) ||
         lg1 == kThreePass)
       return build_three_pass(p, n, batch, in_off, out_off);
@@ -1038,13 +1045,16 @@ float time_group(mcfftPlan p, size_t first, void* a, void* b, void* c, int64_t i
 // whose factor exceeds the tile kernels' range runs a direct-load pass, and
 // the timing decides between it and three tile passes: the four-step pair
 // of 2^25 and 2^26 points has such a factor (8192), the three-pass plan
-// does not.  The choice is recorded as wisdom ("fourstep" records: lg n1,
-// or -1 for three passes) and reported in mcfftPlanInfo.fourstep_n1.
+// does not.  Where the form has a pass of two columns per tile (plain 8192,
+// split 4096) that single pass is the default and the splits are timed
+// against it.  The choice is recorded as wisdom ("fourstep" records: lg n1,
+// -1 for three passes, -2 for one pass) and reported in
+// mcfftPlanInfo.fourstep_n1 (0 for one pass).
 // MCFFT_AUTOTUNE=0, MCFFT_FOURSTEP_N1 or MCFFT_THREE_PASS keep the default
 // (or the forced plan).
 int tune_fourstep(mcfftPlan p, int64_t n, int64_t batch, int64_t in_off, int64_t out_off) {
   const int lg = ilog2(n), def = default_lg1(p, n);
-  if (n <= max_one_pass(p) || n > kMaxSinglePass * kMaxSinglePass) return 0;
+  if (n <= max_four_column(p) || n > kMaxSinglePass * kMaxSinglePass) return 0;
   if (std::getenv("MCFFT_FOURSTEP_N1") || std::getenv("MCFFT_THREE_PASS")) return 0;
   if (const char* e = std::getenv("MCFFT_AUTOTUNE"))
     if (std::atoi(e) == 0) return 0;
@@ -1077,6 +1087,7 @@ int tune_fourstep(mcfftPlan p, int64_t n, int64_t batch, int64_t in_off, int64_t
       cands.push_back(lg1);
   }
   if (lg >= 21 && def != kThreePass) cands.push_back(kThreePass);
+  if (n <= max_one_pass(p) && def != kOnePass) cands.push_back(kOnePass);
   float best_t = -1.f, def_t = -1.f;
   int best = def;
   for (int cand : cands) {
@@ -1097,6 +1108,9 @@ int tune_fourstep(mcfftPlan p, int64_t n, int64_t batch, int64_t in_off, int64_t
       if (cand == kThreePass)
         fprintf(stderr, "[mcfft] tune 1D n=%lld: three passes (%zu launches) %.4f ms\n",
                 (long long)n, npasses, t);
+      else if (cand == kOnePass)
+        fprintf(stderr, "[mcfft] tune 1D n=%lld: one pass (%d tiled) %.4f ms\n", (long long)n,
+                tiled, t);
       else
         fprintf(stderr, "[mcfft] tune 1D n=%lld: n1=%lld (%d of 2 passes tiled) %.4f ms\n",
                 (long long)n, (long long)(int64_t(1) << cand), tiled, t);
@@ -2016,9 +2030,9 @@ mcfftResult mcfftWisdomImport(const char* path) {
     char* end = nullptr;
     const long tp = std::strtol(v.c_str(), &end, 10);
     // tile-shape records hold 8192 or 16384 points; four-step records lg n1
-    // (4..13) or -1 (three passes)
+    // (4..13), -1 (three passes) or -2 (one two-column pass)
     const bool fs = l.find("\tfourstep ") != std::string::npos;
-    const bool fs_ok = (tp >= 4 && tp <= 13) || tp == kThreePass;
+    const bool fs_ok = (tp >= 4 && tp <= 13) || tp == kThreePass || tp == kOnePass;
     if (v.empty() || *end || (fs ? !fs_ok : (tp != 8192 && tp != 16384))) {
       ok = false;
       break;
