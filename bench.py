@@ -649,7 +649,9 @@ def main(argv=None):
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="c2", choices=sorted(CONFIGS))
-    ap.add_argument("--uneven-order", default="sorted", choices=["draw", "sorted", "shuffled"])
+    # the uneven batch's descriptors as drawn (the plan groups them by shape
+    # whatever their order); "sorted" hands them over already grouped
+    ap.add_argument("--uneven-order", default="draw", choices=["draw", "sorted", "shuffled"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline and error legs")
     ap.add_argument("--no-uneven", action="store_true", help="skip the uneven-batch leg")
     args = ap.parse_args(argv)
