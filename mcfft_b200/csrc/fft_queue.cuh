@@ -302,12 +302,28 @@ __device__ __forceinline__ void producer_loop(const QArgs& a, uint32_t sS0, uint
   };
   int64_t il = 0, is = 0;  // next local item to load / to store
   int64_t sig = -1;        // stored item whose completion is still to be signalled
+  QItem sig_it{0u, 0u};    // that item
   bool idle = false;       // no progress since idle_since (global timer, ns)
   uint32_t idle_since = 0;
+  // Item il, read one load ahead so that its latency overlaps the wait for
+  // the consumers (a stored item is read back from its ring slot).
+  QItem nxt = nlocal > 0 ? a.items[blockIdx.x] : QItem{0u, 0u};
+  bool nxt_ready = false;  // item il's dependency seen complete (counters only grow)
+  // Acquire check of item il's dependency: once seen complete it stays so.
+  auto dep_met = [&]() -> bool {
+    if (nxt_ready) return true;
+    const QPass& P = a.pass[nxt.pass];
+    if (P.wait_base >= 0) {
+      if (queue::ld_acquire(a.counters + P.wait_base + nxt.tile / P.col_blocks) < P.wait_count)
+        return false;
+      queue::fence_proxy_async_global();
+    }
+    nxt_ready = true;
+    return true;
+  };
   // Completion of a producing tile: its bulk store has finished writing,
   // then a release add on every key it covers.
-  auto signal = [&](int64_t k) {
-    const QItem it = a.items[blockIdx.x + k * G];
+  auto signal = [&](const QItem& it) {
     const QPass& P = a.pass[it.pass];
     tile::tma_store_wait_all();
     queue::fence_proxy_async_global();
@@ -320,7 +336,7 @@ __device__ __forceinline__ void producer_loop(const QArgs& a, uint32_t sS0, uint
   while (is < nlocal) {
     bool moved = false;
     if (is < il && queue::mbar_test(&outrdy[is & 1], (uint32_t)(is >> 1) & 1u)) {
-      const QItem it = a.items[blockIdx.x + is * G];
+      const QItem it = ring_item(full, (int)(is & 1));  // item is, written when it was loaded
       const QPass& P = a.pass[it.pass];
       const uint32_t src = (is & 1) ? sS1 : sS0;
       const int64_t cb = it.tile % P.col_blocks, outer = it.tile / P.col_blocks;
@@ -334,21 +350,17 @@ __device__ __forceinline__ void producer_loop(const QArgs& a, uint32_t sS0, uint
         tile::tma_store_pol(&P.tmap_out, P.out_ndims, crd, src, pol(P.l2_out));
       }
       tile::tma_store_wait_read();
-      if (sig >= 0) signal(sig);
+      if (sig >= 0) signal(sig_it);
       sig = P.sig_base >= 0 ? is : -1;
+      sig_it = it;
       ++is;
       moved = true;
     }
     if (il < nlocal && il < is + 2 && !*abort_flag) {
-      const QItem it = a.items[blockIdx.x + il * G];
+      const QItem it = nxt;
       const QPass& P = a.pass[it.pass];
       const int64_t outer = it.tile / P.col_blocks;
-      bool ready = true;
-      if (P.wait_base >= 0) {
-        ready = queue::ld_acquire(a.counters + P.wait_base + outer) >= P.wait_count;
-        if (ready) queue::fence_proxy_async_global();
-      }
-      if (ready) {
+      if (dep_met()) {
         const uint32_t dst = (il & 1) ? sS1 : sS0;
         const int64_t cb = it.tile % P.col_blocks;
         volatile QItem* ring = item_ring(full);
@@ -364,7 +376,10 @@ __device__ __forceinline__ void producer_loop(const QArgs& a, uint32_t sS0, uint
                             X && X->in_otab ? X->in_otab[outer] : outer, crd);
           tile::tma_load_pol(&P.tmap_in, P.in_ndims, crd, dst, &full[il & 1], pol(P.l2_in));
         }
+        tile::prefetch_tmap(&P.tmap_out);  // for this tile's store
         ++il;
+        if (il < nlocal) nxt = a.items[blockIdx.x + il * G];
+        nxt_ready = false;
         moved = true;
       }
     }
@@ -372,15 +387,21 @@ __device__ __forceinline__ void producer_loop(const QArgs& a, uint32_t sS0, uint
     // for the store's completion does not delay it (and never later: the
     // next load may depend on this very tile).
     if (sig >= 0) {
-      signal(sig);
+      signal(sig_it);
       sig = -1;
     }
     if (moved) {
       idle = false;
     } else if (is < il && (il == is + 2 || il == nlocal || *abort_flag)) {
-      // Only the consumers' release of tile `is` can make progress: wait for
-      // it on the barrier (a bounded try-wait suspends the thread instead of
-      // spinning, which would take issue slots from the consumers).
+      // Only the consumers' release of tile `is` can make progress: check
+      // the next load's dependency now (its latency then overlaps the
+      // wait), then wait for the release on the barrier (a bounded try-wait
+      // suspends the thread instead of spinning, which would take issue
+      // slots from the consumers).
+      if (il < nlocal && !*abort_flag) {
+        tile::prefetch_tmap(&a.pass[nxt.pass].tmap_in);
+        dep_met();
+      }
       if (!sm100::mbar_wait_bounded(&outrdy[is & 1], (uint32_t)(is >> 1) & 1u, kWaitLimit) ||
           *abort_flag) {
         *abort_flag = 1;
@@ -400,7 +421,7 @@ __device__ __forceinline__ void producer_loop(const QArgs& a, uint32_t sS0, uint
       __nanosleep(128);
     }
   }
-  if (sig >= 0) signal(sig);
+  if (sig >= 0) signal(sig_it);
   tile::tma_store_wait_all();
   // Loads issued but not consumed (abort path) must land before the
   // CTA's shared memory is released.

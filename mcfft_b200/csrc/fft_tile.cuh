@@ -99,6 +99,12 @@ __device__ __forceinline__ void sts64(uint32_t addr, float2 v) {
   asm volatile("st.shared.v2.f32 [%0], {%1,%2};" ::"r"(addr), "f"(v.x), "f"(v.y) : "memory");
 }
 
+// Brings a tensor map (a kernel parameter's generic address) into the
+// descriptor cache ahead of the copy that uses it.
+__device__ __forceinline__ void prefetch_tmap(const CUtensorMap* map) {
+  asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(map)) : "memory");
+}
+
 // TMA bulk-tensor load / store of one tile; coordinates from the recipe.
 __device__ __forceinline__ void tma_load(const CUtensorMap* map, int nd, const int32_t* crd,
                                          uint32_t dst, uint64_t* bar) {
