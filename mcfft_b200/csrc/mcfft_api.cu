@@ -151,6 +151,10 @@ struct mcfftPlan_st {
   bool indexed = false;
   // Four-step split n1 = 2^fs_lg1 of the 1D group being built (0: default).
   int fs_lg1 = 0;
+  // Programmatic dependent launch of the second and later tile passes of
+  // an exec (their setup overlaps the previous pass's last tiles);
+  // MCFFT_PDL=0 at plan creation launches every pass in plain stream order.
+  bool pdl = true;
   // Executable graphs of recent execs, keyed by (in, out, direction): an
   // exec repeated on the same buffers replays its captured launches.
   struct GraphEntry {
@@ -920,6 +924,7 @@ mcfftResult plan_begin(mcfftPlan* out, mcfftPrecision prec, unsigned flags, mcff
   p->prec = prec;
   if (const char* e = std::getenv("MCFFT_GRAPH")) p->graphs_on = std::atoi(e) != 0;
   if (std::getenv("MCFFT_DEBUG_SYNC")) p->graphs_on = false;
+  if (const char* e = std::getenv("MCFFT_PDL")) p->pdl = std::atoi(e) != 0;
   p->flags = flags;
   p->info.precision = (int)prec;
   mcfftResult r = plan_alloc(p, &p->status, sizeof(int));
@@ -1576,24 +1581,13 @@ mcfftResult exec_graph(mcfftPlan p, const void* in, void* out, int dir, cudaStre
   return MCFFT_SUCCESS;
 }
 
-// Programmatic dependent launch of a plan's later tile passes (their setup
-// overlaps the previous pass's last tiles); MCFFT_PDL=0 launches every pass
-// in plain stream order.
-bool pdl_on() {
-  static const bool on = [] {
-    const char* e = std::getenv("MCFFT_PDL");
-    return !e || std::atoi(e) != 0;
-  }();
-  return on;
-}
-
 // One pass on the stream: `src` and `dst` are its input and output with
 // the pass's element offsets already applied.  `follows`: a pass of the
 // same exec ran just before on the stream.
 cudaError_t launch_one(mcfftPlan p, const Pass& ps, const void* src, void* dst, int dir,
                        cudaStream_t st, bool follows) {
   if (ps.tiled) {
-    cudaError_t e = launch_tile_pass(ps.tp, src, dst, dir, st, follows && pdl_on());
+    cudaError_t e = launch_tile_pass(ps.tp, src, dst, dir, st, follows && p->pdl);
     if (e == cudaSuccess && std::getenv("MCFFT_DEBUG_SYNC")) {
       e = cudaStreamSynchronize(st);
       fprintf(stderr, "[mcfft] tile pass L=%d R=%d C=%d grid=%d tiles=%lld: %s\n", ps.tp.k->L,

@@ -67,6 +67,25 @@ def test_malformed_file_refused_and_changes_nothing(tmp_path, text):
     assert records(out) == [RECS[2]]
 
 
+FS = "NVIDIA B200\t148\tfourstep n%d b1 p0 f0\t%s"
+
+
+def test_decomposition_records(tmp_path):
+    """1D decomposition records: lg n1 of a four-step split (4..13), -1 for
+    three passes, -2 for one two-column pass; nothing else."""
+    good = [FS % (1 << 20, "10"), FS % (1 << 24, "-1"), FS % (8192, "-2")]
+    mc.wisdom_import(write(tmp_path / "w.txt", HEADER + "".join(r + "\n" for r in good)))
+    out = tmp_path / "out.txt"
+    mc.wisdom_export(str(out))
+    assert records(out) == good
+    for bad in ("3", "14", "-3", "0", "16384"):
+        with pytest.raises(mc.McfftError) as ei:
+            mc.wisdom_import(write(tmp_path / "bad.txt", HEADER + FS % (1 << 20, bad) + "\n"))
+        assert ei.value.code == mc.INVALID_VALUE
+    mc.wisdom_export(str(out))
+    assert records(out) == good
+
+
 def test_missing_file_and_forget(tmp_path):
     with pytest.raises(mc.McfftError):
         mc.wisdom_import(str(tmp_path / "nope.txt"))
