@@ -472,10 +472,12 @@ bool build(PassLayout* pl, int L, int R, int C, Kind in_kind, Kind out_kind, int
   p.NST = nst;
   if ((1 << (4 * nst)) * R != L || nst < 1) { *err = "L is not 16^a * R"; return false; }
   // Column staging puts min(C, 128 / elem) columns innermost in its TMA box,
-  // which must span 16 bytes: C >= 4.  Row staging's innermost box
+  // which must span 16 bytes: C >= 4 for FP16.  Row staging's innermost box
   // dimension is points (128 bytes), so a row-in / row-out pass also takes
-  // two columns (L = 4096 in 8K-point tiles).
-  const int cmin = in_kind == ROW && out_kind == ROW ? 2 : 4;
+  // two columns (L = 4096 in 8K-point tiles), and so does a row-in pass
+  // whose column output is FP32 (two columns: 16 bytes).  Column input
+  // keeps four columns.
+  const int cmin = in_kind == ROW && (out_kind == ROW || 2 * out_elem >= 16) ? 2 : 4;
   if (C < cmin || (C & (C - 1))) {
     *err = "C must be a power of two >= 4 (>= 2 for row passes)";
     return false;

@@ -98,3 +98,20 @@ def test_three_pass_choice_from_wisdom(tmp_path):
         assert rel < 1e-3, rel
     finally:
         mc.wisdom_forget()
+
+
+@pytest.mark.parametrize("n,n1,batch", [(1 << 22, 1024, 2), (1 << 23, 2048, 1)])
+def test_split_four_step_with_4096_point_rows(n, n1, batch, monkeypatch):
+    """Split form, four-step pairs whose second pass has 4096-point rows
+    (two columns per 8K-point tile, FP32 column output): both passes on the
+    tile kernels, within the split form's tolerance."""
+    monkeypatch.setenv("MCFFT_FOURSTEP_N1", str(n1))
+    x = rand_complex((batch, n), seed=n1 + batch)
+    with mc.Plan((n,), batch, mc.PREC_SPLIT) as p:
+        info = p.info()
+        assert info.num_passes == 2 and info.fourstep_n1 == n1
+        assert info.tile_points == 8192
+        y, _ = run(p, x, False)
+    ref = oracle.fft1d(rounded(x, False))
+    rel, _ = compare(y, ref)
+    assert rel < 2e-6, rel

@@ -94,21 +94,26 @@ def test_split_layouts(checker, L, R, C, ik, ok, ie):
 
 
 @pytest.mark.parametrize("ie", [8, 4])
-def test_split_two_column_row_layout(checker, ie):
-    """Split form, L = 4096 in 8K-point tiles (two columns): row-in /
-    row-out only, FP32 or FP16 input staging, FP32 output; tables
-    consistent and the epilogue conflict-free.  Column staging is refused."""
-    r = subprocess.run([checker, "4096", "1", "2", "row", "row", str(ie), "8"],
+@pytest.mark.parametrize("ok", ["row", "col"])
+def test_split_two_column_row_layout(checker, ie, ok):
+    """Split form, L = 4096 in 8K-point tiles (two columns): row input (FP32
+    or FP16 staging) with row or column FP32 output (two FP32 columns span
+    the 16-byte TMA box); tables consistent and the epilogue conflict-free.
+    Column input is refused (FP16 columns would span 8 bytes)."""
+    r = subprocess.run([checker, "4096", "1", "2", "row", ok, str(ie), "8"],
                        capture_output=True, text=True, timeout=120)
     assert r.returncode == 0, r.stdout + r.stderr
     out = dict(line.split(None, 1) for line in r.stdout.splitlines())
     assert out["tables_consistent"] == "1"
     assert out["epilogue_consistent"] == "1"
     assert float(out["epilogue_excess"]) == pytest.approx(0.0, abs=1e-9)
-    for ik, ok in (("col", "col"), ("row", "col")):
-        r = subprocess.run([checker, "4096", "1", "2", ik, ok, str(ie), "8"], capture_output=True,
-                           text=True, timeout=120)
-        assert r.returncode == 1 and r.stdout.startswith("error"), r.stdout
+    r = subprocess.run([checker, "4096", "1", "2", "col", "col", str(ie), "8"], capture_output=True,
+                       text=True, timeout=120)
+    assert r.returncode == 1 and r.stdout.startswith("error"), r.stdout
+    # FP16 column output (the plain form) keeps four columns
+    r = subprocess.run([checker, "4096", "1", "2", "row", "col", "4", "4"], capture_output=True,
+                       text=True, timeout=120)
+    assert r.returncode == 1 and r.stdout.startswith("error"), r.stdout
 
 
 @pytest.mark.parametrize("C,ie,oe", [(1024, 4, 4), (512, 4, 4), (512, 8, 8), (512, 4, 8)])
