@@ -27,8 +27,12 @@ def test_reference_arm_json_line():
     r = _bench({})
     assert r.returncode == 0, r.stderr
     line = json.loads(r.stdout.strip().splitlines()[-1])
-    with open(os.path.join(ROOT, "BASELINE.json")) as f:
-        assert line["metric"] == json.load(f)["metric"]
+    # the GPU arm's metric (bench.METRIC), read from the script's source so
+    # that nothing here imports torch
+    with open(os.path.join(ROOT, "bench.py")) as f:
+        src = f.read()
+    metric = src.split('METRIC = "', 1)[1].split('"', 1)[0]
+    assert line["metric"] == metric
     assert line["impl"] == "reference"
     assert line["unit"] == "GFLOP/s" and line["value"] > 0 and line["higher_is_better"] is True
     assert line["n_gpus"] == 1 and line["steps"] == 1 and line["warmup"] >= 3
