@@ -87,18 +87,23 @@ def test_gpu_norms_match_oracle(f16):
 # ----------------------------------------------------------- c2: 2^20 x 64
 
 
-@pytest.mark.parametrize("form", ["plain", "split"])
+@pytest.mark.parametrize("form", ["plain", "split", "split_fp32"])
 def test_c2_every_transform(form):
     dims, batch, seed, _ = W.CONFIGS["c2"]
     n = dims[0]
     x = W.uniform((batch, n), seed)
-    xr = rounded(x, True)  # FP16 input in both forms (split: FLAG_INPUT_F16)
-    xd = to_device(x, True)
+    # FP16 input in the plain form and the split form with FLAG_INPUT_F16;
+    # FP32 input in the split form's FP32 in / FP32 out case
+    in16 = form != "split_fp32"
+    xr = rounded(x, in16)
+    xd = to_device(x, in16)
     del x
     if form == "plain":
         p = mc.Plan(dims, batch, mc.PREC_FP16)
-    else:
+    elif form == "split":
         p = mc.Plan(dims, batch, mc.PREC_SPLIT, mc.FLAG_INPUT_F16)
+    else:
+        p = mc.Plan(dims, batch, mc.PREC_SPLIT)
     with p:
         y, info = _exec(p, xd, form == "plain")
     ref = oracle.fft1d(xr)
