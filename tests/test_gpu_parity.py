@@ -110,11 +110,16 @@ def test_split_inverse_roundtrip(shape):
     assert rel_rt < 4 * SPLIT_TOL, rel_rt
 
 
-def test_plain_inverse():
-    x = rand_complex((8, 1024), seed=5)
-    with mc.Plan((1024,), 8, mc.PREC_FP16) as p:
+@pytest.mark.parametrize("shape,batch", [((1024,), 8), ((8192,), 6), ((1 << 24,), 1),
+                                         ((16, 512), 4), ((256, 8192), 1)])
+def test_plain_inverse(shape, batch):
+    """Inverse transforms, plain form: one pass, the 8192-point pass with its
+    computed radix-2 twiddles, three passes (2^24), a 16-point column pass,
+    rows of 8192."""
+    x = rand_complex((batch,) + shape, seed=5)
+    with mc.Plan(shape, batch, mc.PREC_FP16) as p:
         y, sl = run(p, x, True, direction=mc.INVERSE)
-    ref = oracle.fft1d(rounded(x, True), sign=+1) * 2.0 ** sl
+    ref = oracle.fftnd(rounded(x, True), list(shape), sign=+1) * 2.0 ** sl
     rel, _ = compare(y, ref)
     assert rel < PLAIN_TOL, rel
 
